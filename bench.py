@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FDTD engine on the plain large solve.
+
+Workload (one GPU): uniform 512^3 lines, 0.5 mm, 40 seeded boxes (20 PEC,
+20 dielectric eps_r ~ U[2,10]), Mur ABC on +-x/+-y, 8-cell UPML on +-z, TFSF
+Gaussian plane wave f0 = 10 GHz fc = 5 GHz at normal incidence, NF2FF box 10
+cells inside with 3 frequencies (workloads.large_plain).  Synthetic, seeded.
+
+A step is one pass of the reference orchestrator's loop body
+(scripts/lib/sim-engine.mjs:648-681): iterate(100) timesteps, then the lagged
+energy readback.  Metric: MCells/s = cells x timesteps / device time.
+
+Multi-GPU: replicas only (independent solves, no collective); value is the
+sum over ranks of cells x timesteps over the max-over-ranks device time.
+
+--impl reference times the reference's CPU algorithm (the oracle port of
+CPUFDTDEngine, js arithmetic, all host threads) on a bounded sample of the
+same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BATCH = 100          # timesteps per step (the orchestrator's readback interval)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--n", type=int, default=512, help="grid lines per axis")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-timesteps", type=int, default=2, help="timesteps per reference-arm step")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def build_job(n, rank, world, barrier):
+    """Rank 0 builds the seeded job; other ranks load rank 0's copy."""
+    from efs_b200 import workloads
+    if world == 1:
+        return workloads.large_plain(n)
+    path = os.path.join(tempfile.gettempdir(), "efs_bench_job_%d.pkl" % n)
+    import pickle
+    if rank == 0:
+        job = workloads.large_plain(n)
+        with open(path + ".tmp", "wb") as f:
+            pickle.dump(job, f, protocol=4)
+        os.replace(path + ".tmp", path)
+    barrier()
+    if rank != 0:
+        with open(path, "rb") as f:
+            job = pickle.load(f)
+    return job
+
+
+class Clocks:
+    """nvidia-smi sampler running across the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the core kernels from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "core_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    out = {}
+    for line in open(p):
+        f = line.split()
+        if len(f) == 3 and not line.startswith("#"):
+            out[f[0]] = (float(f[1]), int(f[2]))   # kernel -> (bytes per launch, cells of the captured grid)
+    return out
+
+
+def cpu_sample(job, mode, timesteps):
+    """Time the CPU oracle on `timesteps` steps of `job` (all host threads)."""
+    from oracle import oracle
+    from efs_b200 import workloads
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    e = oracle.OracleEngine(mode=mode)
+    workloads.configure(e, dict(job, probes=[]))
+    e.iterate(1)   # first-touch / page-in outside the sample
+    t = time.perf_counter()
+    e.iterate(timesteps)
+    dt = time.perf_counter() - t
+    N = job["grid"][0] * job["grid"][1] * job["grid"][2]
+    return N * timesteps / dt / 1e6, threads, dt
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    from efs_b200 import workloads
+    job = workloads.large_plain(args.n)
+    from oracle import oracle
+    from efs_b200 import workloads as wl
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    e = oracle.OracleEngine(mode="js")
+    wl.configure(e, dict(job, probes=[]))
+    N = job["grid"][0] * job["grid"][1] * job["grid"][2]
+    for _ in range(args.warmup):
+        e.iterate(args.ref_timesteps)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        e.iterate(args.ref_timesteps)
+    dt = time.perf_counter() - t
+    value = N * args.ref_timesteps * args.steps / dt / 1e6
+    sample = "%d timesteps of the %d^3 workload per step (CPUFDTDEngine arithmetic, %d threads)" % (
+        args.ref_timesteps, args.n, threads)
+    print(json.dumps({
+        "impl": "reference", "metric": "MCells/s", "value": round(value, 3), "unit": "MCells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * dt / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": "large_plain %d^3: 40 boxes, Mur +-x/+-y, UPML8 +-z, TFSF, NF2FF F=3" % args.n,
+                   "cells": N, "timesteps_per_step": args.ref_timesteps},
+        "cpu_baseline": {"value": round(value, 3), "unit": "MCells/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "MCells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_b200(args):
+    import torch
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        barrier = lambda: dist.barrier()
+    else:
+        barrier = lambda: None
+    from efs_b200.build import build
+    if rank == 0:
+        build()
+    barrier()
+    from efs_b200.engine import CudaEngine
+    from efs_b200 import workloads
+
+    job = build_job(args.n, rank, world, barrier)
+    N = job["grid"][0] * job["grid"][1] * job["grid"][2]
+    eng = CudaEngine(device=local)
+    assert eng.initGPU(), "no CUDA device"
+    workloads.configure(eng, dict(job, probes=[]))
+    stream = torch.cuda.ExternalStream(eng.stream)
+
+    def step():
+        eng.iterate(BATCH)
+        eng.computeEnergy()          # lagged readback, as the orchestrator does every 100 steps
+
+    for _ in range(args.warmup):
+        step()
+    eng.sync()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    eng.sync()
+    barrier()
+    torch.cuda.synchronize()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    steps_total = args.steps * BATCH
+    value = world * N * steps_total / (ms_max / 1e3) / 1e6
+
+    # dominant kernels timed alone with CUDA events on the engine stream
+    core_ms = eng.timeCore(20)
+    bytes_core = 52.0 * N                    # fused-step algorithmic minimum: 48 B fields + 4 B index
+    t_core = (core_ms[0] + core_ms[1]) / 1e3
+    peak, peak_kind = peaks()
+    achieved = bytes_core / t_core / 1e9
+    traffic = None
+    tr = profiled_traffic()
+    if tr:
+        tot = sum(b * N / cells for k, (b, cells) in tr.items())
+        traffic = tot
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "kernel": "core E+H update (%s), %.1f B/cell algorithmic" % ("two launches" if core_ms[1] > 0 else "fused", 52.0),
+            "ms_per_launch": [round(core_ms[0], 4), round(core_ms[1], 4)], "peak_kind": "of " + peak_kind}
+    step_bytes = workloads.job_bytes_per_step(job)
+    # our kernels in the timed region: per timestep plan + one counter update per
+    # captured graph (64 steps each) + the two energy-reduction kernels per step
+    launches = args.steps * (BATCH * eng.kernelsPerStep() + math.ceil(BATCH / 64) + 2)
+    eng.destroy()
+
+    # end to end through the public API from host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        torch.cuda.synchronize()
+        h2d = 0
+        for k, v in job["coefficients"].items():
+            h2d += np.asarray(v).nbytes
+        for r in job.get("pml") or []:
+            h2d += sum(np.asarray(r[k]).nbytes for k in ("vv", "vvfo", "vvfn", "ii", "iifo", "iifn"))
+        t0 = time.perf_counter()
+        g = CudaEngine(device=local)
+        g.initGPU()
+        workloads.configure(g, dict(job, probes=[]))
+        for _ in range(args.steps):
+            g.iterate(BATCH)
+            g.computeEnergy()
+        acc = g.readNF2FFAccumulation(True)
+        en = g.flushEnergy()
+        g.destroy()
+        dt = time.perf_counter() - t0
+        d2h = (acc["accumE"].nbytes + acc["accumH"].nbytes + 8 * (args.steps + 1)) if acc else 8 * args.steps
+        e2e = {"value": round(N * steps_total / dt / 1e6, 3), "unit": "MCells/s",
+               "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+               "wall_s": round(dt, 3)}
+        del en
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, threads, dt = cpu_sample(job, "js", 2)
+        cpu = {"value": round(v, 3), "unit": "MCells/s", "cores": threads, "kind": "port",
+               "sample": "2 timesteps of the same %d^3 job on the CPU oracle (CPUFDTDEngine arithmetic), %.1f s" % (args.n, dt)}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "MCells/s", "value": round(value, 3), "unit": "MCells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy default_rng(2))",
+            "config": {"workload": "large_plain %d^3: 40 boxes, Mur +-x/+-y, UPML8 +-z, TFSF, NF2FF F=3" % args.n,
+                       "cells": N, "timesteps_per_step": BATCH, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (%.1f GB of fields)" % (24 * N / 1e9),
+                       "bytes_per_timestep_algorithmic": step_bytes},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1214 @@
+// efs_engine.cu — host side of the B200 FDTD engine behind include/efs.h.
+//
+// One engine = one grid resident in HBM + one CUDA stream.  A timestep is the
+// reference's phase sequence (CPUFDTDEngine.step, src/webgpu-fdtd.mjs:1129-
+// 1172, with the PBC and NF2FF/gather passes where WebGPUEngine.iterate puts
+// them, src/webgpu-engine.mjs:2448-2499) mapped onto kernels:
+//
+//   steady-state accumulate | ADE(volt) | Mur pre | RLC pre      (sparse)
+//   E update with UPML pre/post fused per cell                   (k_volt)
+//   TFSF(volt) | PBC(volt) | Mur post | excitation | Mur apply | RLC apply
+//   ADE(curr)                                                    (sparse)
+//   H update with UPML pre/post fused per cell                   (k_curr)
+//   TFSF(curr) | PBC(curr) | NF2FF accumulate | probe ring       (sparse)
+//
+// Reads that the reference makes between the UPML pre-update and the core
+// update (ADE, Mur pre) are redirected to the region's flux array, which is
+// what the field holds at that moment, so fusing pre/post into the core
+// kernels keeps the reference's results.  Time-dependent parameters come
+// from a device-resident step counter, so `iterate(n)` replays a captured
+// CUDA graph of the whole step sequence.
+#include "../../include/efs.h"
+#include "efs_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+using namespace efs;
+
+namespace {
+
+thread_local std::string g_create_error = "no error";
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { reset(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct EfsError {
+    efs_status code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(efs_status code, const std::string& msg) { throw EfsError{code, msg}; }
+
+void ck(cudaError_t err, const char* what) {
+    if (err != cudaSuccess) fail(err == cudaErrorMemoryAllocation ? EFS_ERR_OOM : EFS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+inline uint32_t blocks(size_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+}  // namespace
+
+struct efs_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error = "no error";
+    size_t dev_bytes = 0;
+
+    bool inited = false;
+    uint32_t Nx = 0, Ny = 0, Nz = 0;
+    size_t N = 0;
+    DevBuf volt, curr;
+    bool indexed = false;
+    DevBuf mat, table, vv, vi, ii, iv;
+    uint32_t ntable = 0;
+    DevBuf state;            // StepState
+    uint32_t numTS = 0;      // host mirror
+    StepState hstate{};
+
+    // excitation
+    bool exc_on = false;
+    DevBuf exc_target, exc_off, exc_delay, exc_amp, exc_signal;
+    uint32_t exc_groups = 0, exc_len = 0, exc_period = 0;
+
+    // UPML
+    struct Region {
+        uint32_t s[3], n[3];
+        size_t total;
+        DevBuf vv, vvfo, vvfn, ii, iifo, iifn, vflux, cflux;
+    };
+    std::vector<std::unique_ptr<Region>> pml;
+    DevBuf vflux_ptrs, cflux_ptrs;
+
+    // Mur (host copies kept to rebuild read redirects)
+    bool mur_on = false;
+    std::vector<uint32_t> h_mur_normal, h_mur_shifted;
+    DevBuf mur_coeff, mur_pre_normal, mur_pre_shifted, mur_shifted, mur_apply_target, mur_apply_src, mur_saved;
+    uint32_t mur_n = 0, mur_napply = 0;
+
+    // TFSF
+    bool tfsf_on = false;
+    DevBuf tfsf_signal;
+    uint32_t tfsf_len = 0, tfsf_period = 0;
+    struct PointSet { DevBuf target, off, delay, amp, frac; uint32_t groups = 0; };
+    PointSet tfsf_v, tfsf_c;
+
+    // ADE
+    bool ade_on = false;
+    struct AdeSide {
+        std::vector<uint32_t> h_field;   // dir*N + pos
+        DevBuf src, lorentz, kint, kext, klor, state, lor;
+        uint32_t n = 0;
+    };
+    AdeSide ade_v, ade_c;
+
+    // RLC
+    bool rlc_on = false;
+    DevBuf rlc_gtarget, rlc_goff, rlc_type, rlc_p, rlc_vdn, rlc_jn, rlc_vil;
+    uint32_t rlc_n = 0, rlc_groups = 0;
+    std::vector<uint32_t> rlc_perm;   // device element order -> caller's element order
+
+    // steady state
+    bool ss_on = false, ss_recording = false;
+    DevBuf ss_idx, ss_e1, ss_e2;
+    uint32_t ss_n = 0, ss_period = 0;
+    float ss_threshold = 1e-6f;
+    uint32_t ss_count_before = 0;   // samples taken before the current recording window
+
+    // PBC
+    bool pbc_on = false;
+    struct PbcAxis { uint32_t axis; float c, s; size_t imag_off; };
+    std::vector<PbcAxis> pbc_axes;
+    DevBuf pbc_imag;
+
+    // probes
+    DevBuf gd_idx, gd_out;
+    uint32_t gd_n = 0;
+    bool ring_on = false;
+    DevBuf ring_idx, ring;
+    uint32_t ring_n = 0, ring_max = 0, ring_interval = 1, ring_q0 = 0;
+
+    // NF2FF
+    bool nf_on = false;
+    DevBuf nf_pts, nf_el, nf_E, nf_H;
+    Nf2ffDev nf{};
+
+    // energy (lagged, double-buffered like computeEnergy :2974-3021)
+    DevBuf en_partial, en_result;
+    double* en_host = nullptr;       // pinned, 2 slots
+    cudaEvent_t en_event[2] = {nullptr, nullptr};
+    int en_idx = 0;
+    bool en_pending = false;
+    double en_last = 0.0;
+
+    // graphs
+    bool plan_dirty = true;
+    std::map<uint32_t, cudaGraphExec_t> graphs;
+
+    ~efs_engine() {
+        drop_graphs();
+        for (auto& ev : en_event) if (ev) cudaEventDestroy(ev);
+        if (en_host) cudaFreeHost(en_host);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void drop_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+    void dirty() { plan_dirty = true; drop_graphs(); }
+
+    void alloc(DevBuf& b, size_t bytes, bool zero = true) {
+        b.reset();
+        if (bytes == 0) bytes = 4;
+        ck(cudaMalloc(&b.p, bytes), "cudaMalloc");
+        b.bytes = bytes;
+        if (zero) ck(cudaMemsetAsync(b.p, 0, bytes, stream), "cudaMemsetAsync");
+    }
+    template <typename T>
+    void upload(DevBuf& b, const T* src, size_t n) {
+        alloc(b, n * sizeof(T), false);
+        if (n) ck(cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
+        ck(cudaStreamSynchronize(stream), "upload sync");   // caller may free its buffer on return
+    }
+    template <typename T>
+    void upload(DevBuf& b, const std::vector<T>& v) { upload(b, v.data(), v.size()); }
+
+    void need_init() const { if (!inited) fail(EFS_ERR_STATE, "engine not initialised: call efs_init first"); }
+    void check_idx3(const uint32_t* p, size_t n, const char* what) const {
+        for (size_t i = 0; i < n; ++i)
+            if (p[i] >= 3 * N) fail(EFS_ERR_INVALID, std::string(what) + ": index out of range");
+    }
+
+    Grid grid() const {
+        Grid g;
+        g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.indexed = indexed;
+        g.N = N; g.NyNz = (size_t)Ny * Nz;
+        g.volt = volt.as<float>(); g.curr = curr.as<float>();
+        g.mat = mat.as<uint32_t>(); g.table = table.as<float>();
+        g.vv = vv.as<float>(); g.vi = vi.as<float>(); g.ii = ii.as<float>(); g.iv = iv.as<float>();
+        return g;
+    }
+    PmlSet pml_set() const {
+        PmlSet s;
+        memset(&s, 0, sizeof(s));
+        s.count = (int)pml.size();
+        for (size_t r = 0; r < pml.size(); ++r) {
+            const Region& R = *pml[r];
+            for (int d = 0; d < 3; ++d) { s.r[r].s[d] = R.s[d]; s.r[r].n[d] = R.n[d]; }
+            s.r[r].vv = R.vv.as<float>(); s.r[r].vvfo = R.vvfo.as<float>(); s.r[r].vvfn = R.vvfn.as<float>();
+            s.r[r].ii = R.ii.as<float>(); s.r[r].iifo = R.iifo.as<float>(); s.r[r].iifn = R.iifn.as<float>();
+            s.r[r].vflux = R.vflux.as<float>(); s.r[r].cflux = R.cflux.as<float>();
+        }
+        return s;
+    }
+
+    // Location a read sees after the UPML pre-update: the flux slot of the
+    // last region containing the cell, else the field itself.
+    ReadLoc redirect(uint32_t field_idx) const {
+        uint32_t n = field_idx / (uint32_t)N;
+        size_t cell = field_idx - (size_t)n * N;
+        uint32_t x = (uint32_t)(cell / ((size_t)Ny * Nz));
+        uint32_t y = (uint32_t)((cell / Nz) % Ny);
+        uint32_t z = (uint32_t)(cell % Nz);
+        ReadLoc l{0, field_idx};
+        for (size_t r = 0; r < pml.size(); ++r) {
+            const Region& R = *pml[r];
+            if ((x - R.s[0]) < R.n[0] && (y - R.s[1]) < R.n[1] && (z - R.s[2]) < R.n[2]) {
+                size_t nyz = (size_t)R.n[1] * R.n[2];
+                size_t p = (size_t)n * R.n[0] * nyz + (size_t)(x - R.s[0]) * nyz + (size_t)(y - R.s[1]) * R.n[2] + (z - R.s[2]);
+                l.sel = (uint32_t)r + 1;
+                l.idx = (uint32_t)p;
+            }
+        }
+        return l;
+    }
+
+    // Rebuild everything that depends on more than one configure call.
+    void build_plan() {
+        if (!plan_dirty) return;
+        std::vector<float*> vp, cp;
+        for (auto& r : pml) { vp.push_back(r->vflux.as<float>()); cp.push_back(r->cflux.as<float>()); }
+        if (vp.empty()) { vp.push_back(nullptr); cp.push_back(nullptr); }
+        upload(vflux_ptrs, vp);
+        upload(cflux_ptrs, cp);
+        if (mur_on) {
+            std::vector<ReadLoc> rn(mur_n), rs(mur_n);
+            for (uint32_t i = 0; i < mur_n; ++i) { rn[i] = redirect(h_mur_normal[i]); rs[i] = redirect(h_mur_shifted[i]); }
+            upload(mur_pre_normal, rn);
+            upload(mur_pre_shifted, rs);
+        }
+        for (AdeSide* s : {&ade_v, &ade_c}) {
+            if (!s->n) continue;
+            std::vector<ReadLoc> src(s->n);
+            for (uint32_t i = 0; i < s->n; ++i) src[i] = redirect(s->h_field[i]);
+            upload(s->src, src);
+        }
+        plan_dirty = false;
+    }
+
+    // Enqueue timestep k of a batch (numTS = state.numTS + k).
+    void enqueue_step(uint32_t k) {
+        const Grid g = grid();
+        const PmlSet ps = pml_set();
+        StepState* st = state.as<StepState>();
+        float* V = volt.as<float>();
+        float* C = curr.as<float>();
+        const uint32_t T = 256;
+        const float* const* vfl = vflux_ptrs.as<const float*>();
+        const float* const* cfl = cflux_ptrs.as<const float*>();
+
+        // --- pre-voltage ---
+        if (ss_on)
+            k_steady_state<<<blocks(ss_n, T), T, 0, stream>>>(V, st, k, ss_idx.as<uint32_t>(), ss_n, ss_period,
+                                                              ss_e1.as<float>(), ss_e2.as<float>());
+        if (ade_v.n) k_ade<<<blocks(ade_v.n, T), T, 0, stream>>>(V, ade_dev(ade_v, vfl));
+        MurDev md = mur_dev(vfl);
+        if (mur_on) k_mur_pre<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
+        RlcDev rd = rlc_dev();
+        if (rlc_on) k_rlc_pre<<<blocks(rlc_n, T), T, 0, stream>>>(rd);
+        // --- core E (+UPML) ---
+        dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
+        const bool hp = !pml.empty();
+        if (indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, stream>>>(g, ps); }
+        else { if (hp) k_volt<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, stream>>>(g, ps); }
+        // --- post-voltage / apply ---
+        if (tfsf_on && tfsf_v.groups) k_point_sources<1><<<blocks(tfsf_v.groups, T), T, 0, stream>>>(V, st, k, point_dev(tfsf_v, tfsf_signal, tfsf_len, tfsf_period));
+        if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, true);
+        if (mur_on) k_mur_post<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
+        if (exc_on && exc_groups) {
+            PointSources s{exc_groups, exc_target.as<uint32_t>(), exc_off.as<uint32_t>(), exc_delay.as<uint32_t>(),
+                           exc_amp.as<float>(), nullptr, exc_signal.as<float>(), exc_len, exc_period};
+            k_point_sources<0><<<blocks(exc_groups, T), T, 0, stream>>>(V, st, k, s);
+        }
+        if (mur_on) k_mur_apply<<<blocks(mur_napply, T), T, 0, stream>>>(V, md);
+        if (rlc_on) k_rlc_apply<<<blocks(rlc_groups, T), T, 0, stream>>>(V, rd);
+        // --- pre-current ---
+        if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+        // --- core H (+UPML) ---
+        if (indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, stream>>>(g, ps); }
+        else { if (hp) k_curr<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<false, false><<<cg, cb, 0, stream>>>(g, ps); }
+        // --- post-current ---
+        if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
+        if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, false);
+        // --- after the step ---
+        if (nf_on) k_nf2ff<<<blocks(nf.np, T), T, 0, stream>>>(V, C, st, k, nf);
+        if (ring_on)
+            k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V, C, st, k, ring_idx.as<uint32_t>(), ring_n, ring_interval,
+                                                                  ring_q0, ring_max, ring.as<float>());
+    }
+
+    PointSources point_dev(const PointSet& p, const DevBuf& sig, uint32_t len, uint32_t period) const {
+        return PointSources{p.groups, p.target.as<uint32_t>(), p.off.as<uint32_t>(), p.delay.as<uint32_t>(),
+                            p.amp.as<float>(), p.frac.as<float>(), sig.as<float>(), len, period};
+    }
+    AdeDev ade_dev(const AdeSide& s, const float* const* flux) const {
+        return AdeDev{s.n, s.src.as<ReadLoc>(), s.lorentz.as<uint8_t>(), s.kint.as<float>(), s.kext.as<float>(),
+                      s.klor.as<float>(), s.state.as<float>(), s.lor.as<float>(), flux};
+    }
+    MurDev mur_dev(const float* const* vfl) const {
+        return MurDev{mur_n, mur_napply, mur_coeff.as<float>(), mur_pre_normal.as<ReadLoc>(), mur_pre_shifted.as<ReadLoc>(),
+                      mur_shifted.as<uint32_t>(), mur_apply_target.as<uint32_t>(), mur_apply_src.as<uint32_t>(),
+                      mur_saved.as<float>(), vfl};
+    }
+    RlcDev rlc_dev() const {
+        return RlcDev{rlc_n, rlc_groups, rlc_gtarget.as<uint32_t>(), rlc_goff.as<uint32_t>(), rlc_type.as<uint32_t>(),
+                      rlc_p.as<float>(), rlc_vdn.as<float>(), rlc_jn.as<float>(), rlc_vil.as<float>()};
+    }
+    void launch_pbc(const PbcAxis& a, bool isVolt) {
+        const uint32_t nl[3] = {Nx, Ny, Nz};
+        PbcDev p;
+        p.axis = a.axis; p.volt = isVolt ? 1 : 0;
+        uint32_t t0 = (a.axis + 1) % 3, t1 = (a.axis + 2) % 3;
+        p.fs0 = nl[t0]; p.fs1 = nl[t1];
+        p.b0 = isVolt ? p.fs0 : p.fs0 - 1; p.b1 = isVolt ? p.fs1 : p.fs1 - 1;
+        p.src = isVolt ? nl[a.axis] - 2 : 0; p.dst = isVolt ? 0 : nl[a.axis] - 2;
+        p.Nx = Nx; p.Ny = Ny; p.Nz = Nz; p.cosP = a.c; p.sinP = a.s;
+        p.imag = pbc_imag.as<float>() + a.imag_off;
+        float* F = isVolt ? volt.as<float>() : curr.as<float>();
+        dim3 b(16, 16), gr(blocks(p.b0, 16), blocks(p.b1, 16));
+        if (p.b0 && p.b1) k_pbc<<<gr, b, 0, stream>>>(F, p);
+    }
+
+    void iterate(uint32_t n) {
+        need_init();
+        build_plan();
+        const uint32_t CH = 64;   // steps per captured graph
+        while (n > 0) {
+            uint32_t m = std::min(n, CH);
+            cudaGraphExec_t ge = graph_for(m);
+            ck(cudaGraphLaunch(ge, stream), "cudaGraphLaunch");
+            numTS += m;
+            n -= m;
+        }
+        ck(cudaGetLastError(), "iterate");
+    }
+
+    cudaGraphExec_t graph_for(uint32_t m) {
+        auto it = graphs.find(m);
+        if (it != graphs.end()) return it->second;
+        if (graphs.size() > 8) drop_graphs();
+        cudaGraph_t graph;
+        ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "BeginCapture");
+        try {
+            for (uint32_t k = 0; k < m; ++k) enqueue_step(k);
+            k_advance<<<1, 1, 0, stream>>>(state.as<StepState>(), m);
+        } catch (...) {
+            cudaStreamEndCapture(stream, &graph);
+            throw;
+        }
+        ck(cudaStreamEndCapture(stream, &graph), "EndCapture");
+        cudaGraphExec_t ge;
+        cudaError_t err = cudaGraphInstantiate(&ge, graph, 0);
+        cudaGraphDestroy(graph);
+        ck(err, "cudaGraphInstantiate");
+        graphs[m] = ge;
+        return ge;
+    }
+
+    void sync_state_to_device() {
+        hstate.numTS = numTS;
+        ck(cudaMemcpyAsync(state.p, &hstate, sizeof(StepState), cudaMemcpyHostToDevice, stream), "state upload");
+        ck(cudaStreamSynchronize(stream), "state sync");
+    }
+
+    // group entries by target preserving order: returns unique targets + CSR offsets + permutation
+    static void group_by(const std::vector<uint32_t>& tgt, std::vector<uint32_t>& utarget, std::vector<uint32_t>& off,
+                         std::vector<uint32_t>& perm) {
+        std::unordered_map<uint32_t, uint32_t> first;
+        std::vector<std::vector<uint32_t>> lists;
+        for (uint32_t i = 0; i < tgt.size(); ++i) {
+            auto it = first.find(tgt[i]);
+            if (it == first.end()) { first.emplace(tgt[i], (uint32_t)lists.size()); lists.push_back({i}); utarget.push_back(tgt[i]); }
+            else lists[it->second].push_back(i);
+        }
+        off.assign(1, 0);
+        for (auto& l : lists) { for (uint32_t i : l) perm.push_back(i); off.push_back((uint32_t)perm.size()); }
+    }
+};
+
+namespace {
+
+template <typename F>
+efs_status guard(efs_engine* e, F&& f) {
+    if (!e) return EFS_ERR_INVALID;
+    try {
+        ck(cudaSetDevice(e->device), "cudaSetDevice");
+        f();
+        return EFS_OK;
+    } catch (const EfsError& err) {
+        e->last_error = err.msg;
+        return err.code;
+    } catch (const std::exception& ex) {
+        e->last_error = ex.what();
+        return EFS_ERR_OOM;
+    }
+}
+
+void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
+    if (!dims || dims[0] == 0 || dims[1] == 0 || dims[2] == 0) fail(EFS_ERR_INVALID, "grid dimensions must be positive");
+    size_t N = (size_t)dims[0] * dims[1] * dims[2];
+    if (3 * N >= (1ull << 32)) fail(EFS_ERR_RANGE, "grid too large for 32-bit field indices (3*Nx*Ny*Nz >= 2^32)");
+    // a fresh init drops every extension
+    e->drop_graphs();
+    e->pml.clear();
+    e->exc_on = e->mur_on = e->tfsf_on = e->ade_on = e->rlc_on = e->ss_on = e->pbc_on = e->ring_on = e->nf_on = false;
+    e->ade_v = efs_engine::AdeSide(); e->ade_c = efs_engine::AdeSide();
+    e->gd_n = 0;
+    e->Nx = dims[0]; e->Ny = dims[1]; e->Nz = dims[2]; e->N = N;
+    e->alloc(e->volt, 3 * N * sizeof(float));
+    e->alloc(e->curr, 3 * N * sizeof(float));
+    e->alloc(e->state, sizeof(StepState));
+    e->numTS = 0;
+    e->hstate = StepState{};
+    e->en_pending = false; e->en_last = 0.0; e->en_idx = 0;
+    e->en_partial.reset(); e->en_result.reset();
+    e->vv.reset(); e->vi.reset(); e->ii.reset(); e->iv.reset(); e->mat.reset(); e->table.reset();
+}
+
+// FNV-1a over the 48-byte tuple
+struct TupleHash {
+    size_t operator()(const std::array<uint32_t, 12>& t) const {
+        uint64_t h = 1469598103934665603ull;
+        for (uint32_t w : t) { h ^= w; h *= 1099511628211ull; }
+        return (size_t)h;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+efs_status efs_create(efs_engine** out, int device) {
+    if (!out) return EFS_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t err = cudaGetDeviceCount(&n);
+    if (err != cudaSuccess || n == 0) {
+        g_create_error = std::string("no CUDA device: ") + (err != cudaSuccess ? cudaGetErrorString(err) : "count 0");
+        return EFS_ERR_CUDA;
+    }
+    if (device < 0 || device >= n) { g_create_error = "device index out of range"; return EFS_ERR_INVALID; }
+    auto* e = new efs_engine();
+    e->device = device;
+    try {
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaMallocHost(&e->en_host, 2 * sizeof(double)), "cudaMallocHost");
+        for (auto& ev : e->en_event) ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    } catch (const EfsError& ex) {
+        g_create_error = ex.msg;
+        delete e;
+        return ex.code;
+    }
+    *out = e;
+    return EFS_OK;
+}
+
+efs_status efs_destroy(efs_engine* e) {
+    if (!e) return EFS_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    delete e;
+    return EFS_OK;
+}
+
+const char* efs_last_error(const efs_engine* e) { return e ? e->last_error.c_str() : g_create_error.c_str(); }
+
+efs_status efs_init(efs_engine* e, const uint32_t dims[3], const float* vv, const float* vi, const float* ii, const float* iv) {
+    return guard(e, [&] {
+        if (!vv || !vi || !ii || !iv) fail(EFS_ERR_INVALID, "coefficient arrays must be non-null");
+        alloc_fields(e, dims);
+        const size_t N = e->N;
+        // Deduplicate per-cell (vv,vi,ii,iv) x 3 tuples into a material table.
+        std::unordered_map<std::array<uint32_t, 12>, uint32_t, TupleHash> ids;
+        std::vector<uint32_t> mat(N);
+        std::vector<float> table;
+        const size_t limit = std::min<size_t>(1u << 22, std::max<size_t>(4096, N / 4));
+        bool ok = true;
+        ids.reserve(std::min<size_t>(limit, 1 << 16));
+        for (size_t c = 0; c < N && ok; ++c) {
+            std::array<uint32_t, 12> t;
+            const float* src[4] = {vv, vi, ii, iv};
+            for (int a = 0; a < 4; ++a)
+                for (int n = 0; n < 3; ++n) memcpy(&t[a * 3 + n], src[a] + n * N + c, 4);
+            auto it = ids.find(t);
+            if (it == ids.end()) {
+                if (ids.size() >= limit) { ok = false; break; }
+                uint32_t id = (uint32_t)ids.size();
+                ids.emplace(t, id);
+                for (int q = 0; q < 12; ++q) { float f; memcpy(&f, &t[q], 4); table.push_back(f); }
+                mat[c] = id;
+            } else {
+                mat[c] = it->second;
+            }
+        }
+        if (ok) {
+            e->indexed = true;
+            e->ntable = (uint32_t)ids.size();
+            e->upload(e->mat, mat);
+            e->upload(e->table, table);
+        } else {
+            e->indexed = false;
+            e->upload(e->vv, vv, 3 * N); e->upload(e->vi, vi, 3 * N);
+            e->upload(e->ii, ii, 3 * N); e->upload(e->iv, iv, 3 * N);
+        }
+        e->sync_state_to_device();
+        e->inited = true;
+        e->dirty();
+    });
+}
+
+efs_status efs_init_indexed(efs_engine* e, const uint32_t dims[3], const uint32_t* mat, const float* table, uint32_t ntable) {
+    return guard(e, [&] {
+        if (!mat || !table || ntable == 0) fail(EFS_ERR_INVALID, "mat/table must be non-null and ntable > 0");
+        alloc_fields(e, dims);
+        for (size_t c = 0; c < e->N; ++c)
+            if (mat[c] >= ntable) fail(EFS_ERR_INVALID, "material index out of range");
+        e->indexed = true;
+        e->ntable = ntable;
+        e->upload(e->mat, mat, e->N);
+        e->upload(e->table, table, (size_t)ntable * 12);
+        e->sync_state_to_device();
+        e->inited = true;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_excitation(efs_engine* e, const float* signal, uint32_t L, const uint32_t* delay, const float* amp,
+                                    const uint32_t* dir, const uint32_t* pos, uint32_t count, uint32_t period) {
+    return guard(e, [&] {
+        e->need_init();
+        if (L == 0 || !signal) fail(EFS_ERR_INVALID, "excitation signal must be non-empty");
+        if (count && (!delay || !amp || !dir || !pos)) fail(EFS_ERR_INVALID, "excitation arrays must be non-null");
+        std::vector<uint32_t> tgt(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            if (dir[i] > 2 || pos[i] >= e->N) fail(EFS_ERR_INVALID, "excitation dir/pos out of range");
+            tgt[i] = dir[i] * (uint32_t)e->N + pos[i];
+        }
+        std::vector<uint32_t> ut, off, perm;
+        efs_engine::group_by(tgt, ut, off, perm);
+        std::vector<uint32_t> d(count);
+        std::vector<float> a(count);
+        for (uint32_t i = 0; i < count; ++i) { d[i] = delay[perm[i]]; a[i] = amp[perm[i]]; }
+        e->upload(e->exc_target, ut); e->upload(e->exc_off, off);
+        e->upload(e->exc_delay, d); e->upload(e->exc_amp, a);
+        e->upload(e->exc_signal, signal, L);
+        e->exc_groups = (uint32_t)ut.size(); e->exc_len = L; e->exc_period = period;
+        e->exc_on = true;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region* regions) {
+    return guard(e, [&] {
+        e->need_init();
+        if (count > (uint32_t)MAX_PML) fail(EFS_ERR_RANGE, "too many UPML regions (max 24)");
+        if (count && !regions) fail(EFS_ERR_INVALID, "regions must be non-null");
+        const uint32_t nl[3] = {e->Nx, e->Ny, e->Nz};
+        std::vector<std::unique_ptr<efs_engine::Region>> out;
+        for (uint32_t r = 0; r < count; ++r) {
+            const efs_pml_region& in = regions[r];
+            auto R = std::make_unique<efs_engine::Region>();
+            for (int d = 0; d < 3; ++d) {
+                // wasm-gpu-bridge.mjs:_validatePMLRegion (:206-236)
+                if ((uint64_t)in.start[d] + in.num[d] > nl[d]) fail(EFS_ERR_INVALID, "PML region extends beyond grid");
+                R->s[d] = in.start[d]; R->n[d] = in.num[d];
+            }
+            if (!in.vv || !in.vvfo || !in.vvfn || !in.ii || !in.iifo || !in.iifn) fail(EFS_ERR_INVALID, "PML region array missing");
+            R->total = 3 * (size_t)R->n[0] * R->n[1] * R->n[2];
+            e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
+            e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
+            e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
+            out.push_back(std::move(R));
+        }
+        e->pml = std::move(out);
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_mur(efs_engine* e, const float* coeff, const uint32_t* normal, const uint32_t* shifted, uint32_t n) {
+    return guard(e, [&] {
+        e->need_init();
+        if (n && (!coeff || !normal || !shifted)) fail(EFS_ERR_INVALID, "Mur arrays must be non-null");
+        e->check_idx3(normal, n, "Mur normal_idx");
+        e->check_idx3(shifted, n, "Mur shifted_idx");
+        e->h_mur_normal.assign(normal, normal + n);
+        e->h_mur_shifted.assign(shifted, shifted + n);
+        // apply: last writer per target wins (sequential loop :1016-1023)
+        std::unordered_map<uint32_t, uint32_t> last;
+        std::vector<uint32_t> order;
+        for (uint32_t i = 0; i < n; ++i) {
+            auto it = last.find(normal[i]);
+            if (it == last.end()) { last.emplace(normal[i], i); order.push_back(normal[i]); }
+            else it->second = i;
+        }
+        std::vector<uint32_t> at(order.size()), as(order.size());
+        for (size_t i = 0; i < order.size(); ++i) { at[i] = order[i]; as[i] = last[order[i]]; }
+        e->upload(e->mur_coeff, coeff, n);
+        e->upload(e->mur_shifted, shifted, n);
+        e->upload(e->mur_apply_target, at); e->upload(e->mur_apply_src, as);
+        e->alloc(e->mur_saved, (size_t)n * 4);
+        e->mur_n = n; e->mur_napply = (uint32_t)order.size();
+        e->mur_on = n > 0;
+        e->dirty();
+    });
+}
+
+static void build_points(efs_engine* e, efs_engine::PointSet& ps, const efs_tfsf_point* pts, uint32_t n) {
+    std::vector<uint32_t> tgt(n);
+    for (uint32_t i = 0; i < n; ++i) tgt[i] = pts[i].field_idx;
+    e->check_idx3(tgt.data(), n, "TFSF field_idx");
+    std::vector<uint32_t> ut, off, perm;
+    efs_engine::group_by(tgt, ut, off, perm);
+    std::vector<uint32_t> d(n);
+    std::vector<float> a(n), f(n);
+    for (uint32_t i = 0; i < n; ++i) { d[i] = pts[perm[i]].delay_int; a[i] = pts[perm[i]].amp; f[i] = pts[perm[i]].delay_frac; }
+    e->upload(ps.target, ut); e->upload(ps.off, off); e->upload(ps.delay, d); e->upload(ps.amp, a); e->upload(ps.frac, f);
+    ps.groups = (uint32_t)ut.size();
+}
+
+efs_status efs_configure_tfsf(efs_engine* e, const float* signal, uint32_t L, uint32_t period, const efs_tfsf_point* vp,
+                              uint32_t nv, const efs_tfsf_point* cp, uint32_t nc) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!signal || L == 0) fail(EFS_ERR_INVALID, "TFSF signal must be non-empty");
+        if ((nv && !vp) || (nc && !cp)) fail(EFS_ERR_INVALID, "TFSF point arrays must be non-null");
+        build_points(e, e->tfsf_v, vp, nv);
+        build_points(e, e->tfsf_c, cp, nc);
+        e->upload(e->tfsf_signal, signal, L);
+        e->tfsf_len = L; e->tfsf_period = period;
+        e->tfsf_on = true;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order* orders) {
+    return guard(e, [&] {
+        e->need_init();
+        if (count && !orders) fail(EFS_ERR_INVALID, "orders must be non-null");
+        for (int side = 0; side < 2; ++side) {
+            efs_engine::AdeSide& s = side == 0 ? e->ade_v : e->ade_c;
+            s = efs_engine::AdeSide();
+            std::vector<uint8_t> lor;
+            std::vector<float> ki, ke, kl;
+            for (uint32_t o = 0; o < count; ++o) {
+                const efs_ade_order& od = orders[o];
+                if (od.num_directions && !od.directions) fail(EFS_ERR_INVALID, "ADE directions must be non-null");
+                for (uint32_t d = 0; d < od.num_directions; ++d) {
+                    const efs_ade_direction& dr = od.directions[d];
+                    if (dr.dir > 2 || (od.num_cells && !dr.pos_idx)) fail(EFS_ERR_INVALID, "ADE direction invalid");
+                    const float* a = side == 0 ? dr.v_int : dr.i_int;
+                    const float* b = side == 0 ? dr.v_ext : dr.i_ext;
+                    const float* c = side == 0 ? dr.v_lor : dr.i_lor;
+                    for (uint32_t i = 0; i < od.num_cells; ++i) {
+                        if (dr.pos_idx[i] >= e->N) fail(EFS_ERR_INVALID, "ADE pos_idx out of range");
+                        s.h_field.push_back(dr.dir * (uint32_t)e->N + dr.pos_idx[i]);
+                        lor.push_back(od.has_lorentz ? 1 : 0);
+                        ki.push_back(a ? a[i] : 0.f); ke.push_back(b ? b[i] : 0.f); kl.push_back(c ? c[i] : 0.f);
+                    }
+                }
+            }
+            s.n = (uint32_t)s.h_field.size();
+            e->upload(s.lorentz, lor); e->upload(s.kint, ki); e->upload(s.kext, ke); e->upload(s.klor, kl);
+            e->alloc(s.state, (size_t)s.n * 4); e->alloc(s.lor, (size_t)s.n * 4);
+        }
+        e->ade_on = count > 0;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_rlc(efs_engine* e, uint32_t n, const efs_rlc_element* el) {
+    return guard(e, [&] {
+        e->need_init();
+        if (n && !el) fail(EFS_ERR_INVALID, "elements must be non-null");
+        std::vector<uint32_t> tgt(n), type(n);
+        std::vector<float> p(9 * (size_t)n);
+        for (uint32_t i = 0; i < n; ++i) {
+            if (el[i].direction > 2 || el[i].field_idx >= e->N) fail(EFS_ERR_INVALID, "RLC field_idx/direction out of range");
+            tgt[i] = el[i].direction * (uint32_t)e->N + el[i].field_idx;
+            type[i] = el[i].type_flag;
+            const float v[9] = {el[i].i2v, el[i].ilv, el[i].vvd, el[i].vv2, el[i].vj1, el[i].vj2, el[i].ib0, el[i].b1, el[i].b2};
+            memcpy(&p[9 * (size_t)i], v, sizeof(v));
+        }
+        std::vector<uint32_t> ut, off, perm;
+        efs_engine::group_by(tgt, ut, off, perm);
+        // groups hold element ids in original order; state stays per element
+        std::vector<uint32_t> goff(off);
+        // k_rlc_apply walks e in [goff[g], goff[g+1]) as element ids: permute element data into group order
+        std::vector<uint32_t> type2(n);
+        std::vector<float> p2(9 * (size_t)n);
+        for (uint32_t i = 0; i < n; ++i) { type2[i] = type[perm[i]]; memcpy(&p2[9 * (size_t)i], &p[9 * (size_t)perm[i]], 36); }
+        e->upload(e->rlc_gtarget, ut); e->upload(e->rlc_goff, goff);
+        e->upload(e->rlc_type, type2); e->upload(e->rlc_p, p2);
+        e->alloc(e->rlc_vdn, 3 * (size_t)n * 4); e->alloc(e->rlc_jn, 3 * (size_t)n * 4); e->alloc(e->rlc_vil, (size_t)n * 4);
+        e->rlc_n = n; e->rlc_groups = (uint32_t)ut.size();
+        e->rlc_on = n > 0;
+        // element order on the device is the grouped order; remember it for state reads
+        e->rlc_perm = perm;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_pbc(efs_engine* e, uint32_t count, const uint32_t* axes, const double* phases) {
+    return guard(e, [&] {
+        e->need_init();
+        if (count && !axes) fail(EFS_ERR_INVALID, "axes must be non-null");
+        const uint32_t nl[3] = {e->Nx, e->Ny, e->Nz};
+        e->pbc_axes.clear();
+        size_t off = 0;
+        for (uint32_t i = 0; i < count; ++i) {
+            if (axes[i] > 2 || nl[axes[i]] < 2) fail(EFS_ERR_INVALID, "PBC axis invalid");
+            double ph = phases ? phases[i] : 0.0;
+            uint32_t t0 = (axes[i] + 1) % 3, t1 = (axes[i] + 2) % 3;
+            size_t fs = (size_t)nl[t0] * nl[t1];
+            e->pbc_axes.push_back({axes[i], (float)std::cos(ph), (float)std::sin(ph), ph != 0.0 ? off : 0});
+            if (ph != 0.0) off += 4 * fs;
+        }
+        e->alloc(e->pbc_imag, std::max<size_t>(off, 1) * 4);
+        e->pbc_on = count > 0;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_steady_state(efs_engine* e, const uint32_t* idx, uint32_t n, uint32_t period, float threshold) {
+    return guard(e, [&] {
+        e->need_init();
+        if (n && !idx) fail(EFS_ERR_INVALID, "probe_idx must be non-null");
+        e->check_idx3(idx, n, "steady-state probe_idx");
+        e->upload(e->ss_idx, idx, n);
+        e->alloc(e->ss_e1, (size_t)n * 4); e->alloc(e->ss_e2, (size_t)n * 4);
+        e->ss_n = n; e->ss_period = period; e->ss_threshold = threshold > 0 ? threshold : 1e-6f;
+        e->ss_on = n > 0; e->ss_recording = false; e->ss_count_before = 0;
+        e->hstate.ss_recording = 0; e->hstate.ss_start = e->numTS; e->hstate.ss_base = 0;
+        e->sync_state_to_device();
+        e->dirty();
+    });
+}
+
+efs_status efs_set_steady_state_recording(efs_engine* e, int rec) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!e->ss_on) fail(EFS_ERR_STATE, "steady state not configured");
+        bool r = rec != 0;
+        if (r == e->ss_recording) return;
+        if (!r) e->ss_count_before += e->numTS - e->hstate.ss_start;   // close the window
+        e->ss_recording = r;
+        e->hstate.ss_recording = r ? 1 : 0;
+        e->hstate.ss_start = e->numTS;
+        e->hstate.ss_base = e->ss_count_before;
+        e->sync_state_to_device();
+    });
+}
+
+efs_status efs_read_steady_state(efs_engine* e, float* e1, float* e2, uint32_t* cur, int* conv) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!e->ss_on) fail(EFS_ERR_STATE, "steady state not configured");
+        std::vector<float> a(e->ss_n), b(e->ss_n);
+        ck(cudaMemcpyAsync(a.data(), e->ss_e1.p, (size_t)e->ss_n * 4, cudaMemcpyDeviceToHost, e->stream), "read ss");
+        ck(cudaMemcpyAsync(b.data(), e->ss_e2.p, (size_t)e->ss_n * 4, cudaMemcpyDeviceToHost, e->stream), "read ss");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+        uint32_t sample = e->ss_count_before + (e->ss_recording ? e->numTS - e->hstate.ss_start : 0);
+        if (e1) memcpy(e1, a.data(), a.size() * 4);
+        if (e2) memcpy(e2, b.data(), b.size() * 4);
+        if (cur) *cur = sample;
+        if (conv) {
+            // src/webgpu-fdtd.mjs:1076-1092
+            int c = 0;
+            if (sample >= 2 * e->ss_period) {
+                double mr = 0;
+                for (uint32_t i = 0; i < e->ss_n; ++i) {
+                    double x1 = a[i], x2 = b[i];
+                    if (std::fabs(x1) < 1e-30) continue;
+                    mr = std::max(mr, std::fabs(x2 - x1) / std::fabs(x1));
+                }
+                c = mr < e->ss_threshold ? 1 : 0;
+            }
+            *conv = c;
+        }
+    });
+}
+
+efs_status efs_iterate(efs_engine* e, uint32_t n) { return guard(e, [&] { e->iterate(n); }); }
+
+efs_status efs_num_ts(const efs_engine* e, uint32_t* out) {
+    if (!e || !out) return EFS_ERR_INVALID;
+    *out = e->numTS;
+    return EFS_OK;
+}
+
+efs_status efs_sync(efs_engine* e) { return guard(e, [&] { ck(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize"); }); }
+
+efs_status efs_get_stream(efs_engine* e, void** s) {
+    if (!e || !s) return EFS_ERR_INVALID;
+    *s = (void*)e->stream;
+    return EFS_OK;
+}
+
+efs_status efs_configure_probe_gather(efs_engine* e, const uint32_t* idx, uint32_t n) {
+    return guard(e, [&] {
+        e->need_init();
+        if (n == 0) return;   // the reference returns without configuring (:2578)
+        if (!idx) fail(EFS_ERR_INVALID, "indices must be non-null");
+        e->check_idx3(idx, n, "probe index");
+        e->upload(e->gd_idx, idx, n);
+        e->alloc(e->gd_out, 2 * (size_t)n * 4);
+        e->gd_n = n;
+    });
+}
+
+efs_status efs_read_probe_gather(efs_engine* e, float* out, size_t len) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!e->gd_n) fail(EFS_ERR_STATE, "probe gather not configured");
+        if (!out || len < 2 * (size_t)e->gd_n) fail(EFS_ERR_INVALID, "output buffer too small");
+        k_gather<<<blocks(e->gd_n, 64), 64, 0, e->stream>>>(e->volt.as<float>(), e->curr.as<float>(), e->gd_idx.as<uint32_t>(),
+                                                             e->gd_n, e->gd_out.as<float>());
+        ck(cudaGetLastError(), "gather");
+        ck(cudaMemcpyAsync(out, e->gd_out.p, 2 * (size_t)e->gd_n * 4, cudaMemcpyDeviceToHost, e->stream), "read gather");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+efs_status efs_configure_probe_gather_buffered(efs_engine* e, const uint32_t* idx, uint32_t n, uint32_t maxS, uint32_t interval) {
+    return guard(e, [&] {
+        e->need_init();
+        if (n == 0) return;   // :2624
+        if (!idx) fail(EFS_ERR_INVALID, "indices must be non-null");
+        if (interval == 0) fail(EFS_ERR_INVALID, "sample_interval must be > 0");
+        e->check_idx3(idx, n, "probe index");
+        e->upload(e->ring_idx, idx, n);
+        e->alloc(e->ring, (size_t)maxS * n * 2 * 4);
+        e->ring_n = n; e->ring_max = maxS; e->ring_interval = interval;
+        e->ring_q0 = e->numTS / interval;    // multiples already passed at configure time
+        e->ring_on = true;
+        e->dirty();
+    });
+}
+
+efs_status efs_read_probe_gather_buffered(efs_engine* e, float* out, size_t len, uint32_t* ns, uint32_t* stride) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!e->ring_on) fail(EFS_ERR_STATE, "buffered probe gather not configured");
+        uint32_t q = e->numTS / e->ring_interval;
+        uint32_t s = q > e->ring_q0 ? std::min(q - e->ring_q0, e->ring_max) : 0;
+        if (ns) *ns = s;
+        if (stride) *stride = 2 * e->ring_n;
+        if (!out) return;
+        size_t need = (size_t)s * e->ring_n * 2;
+        if (len < need) fail(EFS_ERR_INVALID, "output buffer too small");
+        if (need) ck(cudaMemcpyAsync(out, e->ring.p, need * 4, cudaMemcpyDeviceToHost, e->stream), "read ring");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+efs_status efs_configure_nf2ff(efs_engine* e, const uint32_t* pts, uint32_t np, const double* omegas, uint32_t nf, double dT,
+                               const float* el, uint32_t maxTS, uint32_t window) {
+    return guard(e, [&] {
+        e->need_init();
+        if (np == 0) return;   // :2732
+        if (!pts || !omegas || !el) fail(EFS_ERR_INVALID, "NF2FF arrays must be non-null");
+        if (nf == 0 || nf > (uint32_t)NF_MAX_FREQ) fail(EFS_ERR_RANGE, "NF2FF frequency count must be 1..16");
+        for (uint32_t i = 0; i < np; ++i)
+            if (pts[3 * i] >= e->Nx || pts[3 * i + 1] >= e->Ny || pts[3 * i + 2] >= e->Nz) fail(EFS_ERR_INVALID, "NF2FF point out of grid");
+        e->upload(e->nf_pts, pts, 3 * (size_t)np);
+        size_t nel = 2 * ((size_t)e->Nx + e->Ny + e->Nz);
+        e->upload(e->nf_el, el, nel);
+        e->alloc(e->nf_E, (size_t)nf * np * 6 * 4);
+        e->alloc(e->nf_H, (size_t)nf * np * 6 * 4);
+        Nf2ffDev& d = e->nf;
+        memset(&d, 0, sizeof(d));
+        d.np = np; d.nf = nf; d.maxTS = maxTS; d.window = window;
+        d.Nx = e->Nx; d.Ny = e->Ny; d.Nz = e->Nz;
+        const uint32_t nl[3] = {e->Nx, e->Ny, e->Nz};
+        uint32_t o = 0;
+        for (int k = 0; k < 6; ++k) { d.off[k] = o; o += nl[k % 3]; }
+        d.pts = e->nf_pts.as<uint32_t>(); d.el = e->nf_el.as<float>();
+        d.accE = e->nf_E.as<float>(); d.accH = e->nf_H.as<float>();
+        for (uint32_t f = 0; f < nf; ++f) d.wdt[f] = omegas[f] * dT;
+        d.dT32 = (float)dT;
+        double wn = 1.0;
+        if (window == 1 && maxTS > 1) {   // windowNorm (:2765-2772)
+            double s = 0;
+            for (uint32_t n = 0; n < maxTS; ++n) s += 0.5 * (1 - std::cos(2 * M_PI * n / (double)(maxTS - 1)));
+            wn = 1.0 / s;
+        }
+        d.wnorm = (float)wn;
+        e->nf_on = true;
+        e->dirty();
+    });
+}
+
+efs_status efs_read_nf2ff(efs_engine* e, float* accE, float* accH, size_t len) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!e->nf_on) fail(EFS_ERR_STATE, "NF2FF not configured");
+        size_t n = (size_t)e->nf.nf * e->nf.np * 6;
+        if (len < n) fail(EFS_ERR_INVALID, "output buffer too small");
+        if (accE) ck(cudaMemcpyAsync(accE, e->nf_E.p, n * 4, cudaMemcpyDeviceToHost, e->stream), "read nf2ff E");
+        if (accH) ck(cudaMemcpyAsync(accH, e->nf_H.p, n * 4, cudaMemcpyDeviceToHost, e->stream), "read nf2ff H");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+efs_status efs_far_field(efs_engine* e, uint32_t fi, const float* meta, const float* theta, uint32_t nth, const float* phi,
+                         uint32_t nph, const double center[3], double freq, double radius, float* out) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!e->nf_on) fail(EFS_ERR_STATE, "NF2FF not configured");
+        if (fi >= e->nf.nf) fail(EFS_ERR_INVALID, "frequency index out of range");
+        if (!meta || !theta || !phi || !out || nth == 0 || nph == 0) fail(EFS_ERR_INVALID, "far-field arguments invalid");
+        const uint32_t np = e->nf.np;
+        const uint32_t A = nth * nph;
+        DevBuf dm, dth, dph, dpart, dout;
+        e->upload(dm, meta, 8 * (size_t)np);
+        e->upload(dth, theta, nth);
+        e->upload(dph, phi, nph);
+        // split points so that angle-blocks x chunks covers the SMs a few times
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+        uint32_t ablocks = blocks(A, FF_THREADS);
+        uint32_t chunks = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)(4 * sms) / std::max<uint32_t>(ablocks, 1), blocks(np, FF_TILE)));
+        uint32_t chunk = (uint32_t)(((size_t)np + chunks - 1) / chunks);
+        chunk = ((chunk + FF_TILE - 1) / FF_TILE) * FF_TILE;
+        chunks = std::max<uint32_t>(1, blocks(np, chunk));
+        e->alloc(dpart, (size_t)chunks * A * 8 * 4, false);
+        e->alloc(dout, (size_t)A * 5 * 4, false);
+        const double C0 = 299792458.0;
+        const double k = 2 * M_PI * freq / C0;
+        FarFieldDev d;
+        d.np = np; d.nth = nth; d.nph = nph; d.chunk = chunk;
+        d.k = (float)k; d.cx = (float)center[0]; d.cy = (float)center[1]; d.cz = (float)center[2];
+        d.accE = e->nf_E.as<float>() + (size_t)fi * np * 6;
+        d.accH = e->nf_H.as<float>() + (size_t)fi * np * 6;
+        d.meta = dm.as<float>(); d.theta = dth.as<float>(); d.phi = dph.as<float>(); d.partial = dpart.as<float>();
+        k_far_field<<<dim3(ablocks, chunks), FF_THREADS, 0, e->stream>>>(d);
+        const double fmag = k / (4 * M_PI * radius), fph = -k * radius;   // (:2880-2884)
+        k_far_field_final<<<blocks(A, 256), 256, 0, e->stream>>>(dpart.as<float>(), A, chunks, fmag * (-std::sin(fph)),
+                                                                   fmag * std::cos(fph), dout.as<float>());
+        ck(cudaGetLastError(), "far field");
+        ck(cudaMemcpyAsync(out, dout.p, (size_t)A * 5 * 4, cudaMemcpyDeviceToHost, e->stream), "read far field");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+static void energy_launch(efs_engine* e, int slot) {
+    if (!e->en_partial.p) {
+        e->alloc(e->en_partial, 1024 * sizeof(double));
+        e->alloc(e->en_result, sizeof(double));
+    }
+    double* res = e->en_result.as<double>();
+    if (e->Nx < 2 || e->Ny < 2 || e->Nz < 2) {
+        ck(cudaMemsetAsync(res, 0, sizeof(double), e->stream), "memset");
+    } else {
+        k_energy<<<1024, 256, 0, e->stream>>>(e->volt.as<float>(), e->curr.as<float>(), e->Nx, e->Ny, e->Nz, e->en_partial.as<double>());
+        k_energy_final<<<1, 1024, 0, e->stream>>>(e->en_partial.as<double>(), 1024, res);
+    }
+    ck(cudaGetLastError(), "energy");
+    ck(cudaMemcpyAsync(e->en_host + slot, res, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "energy readback");
+    ck(cudaEventRecord(e->en_event[slot], e->stream), "event");
+}
+
+efs_status efs_energy(efs_engine* e, int lagged, double* out) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
+        if (!lagged) {
+            energy_launch(e, e->en_idx);
+            ck(cudaEventSynchronize(e->en_event[e->en_idx]), "energy wait");
+            *out = e->en_host[e->en_idx];
+            return;
+        }
+        // computeEnergy (:2974-3021): queue this value, return the previous one
+        const int cur = e->en_idx, prev = 1 - cur;
+        energy_launch(e, cur);
+        if (e->en_pending) {
+            ck(cudaEventSynchronize(e->en_event[prev]), "energy wait");
+            e->en_last = e->en_host[prev];
+        }
+        e->en_pending = true;
+        e->en_idx = prev;
+        *out = e->en_last;
+    });
+}
+
+efs_status efs_flush_energy(efs_engine* e, double* out) {
+    return guard(e, [&] {
+        e->need_init();
+        if (e->en_pending) {
+            const int slot = 1 - e->en_idx;   // the slot written by the last lagged call
+            ck(cudaEventSynchronize(e->en_event[slot]), "energy wait");
+            e->en_last = e->en_host[slot];
+            e->en_pending = false;
+        }
+        if (out) *out = e->en_last;
+    });
+}
+
+efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
+    return guard(e, [&] {
+        e->need_init();
+        if (v) ck(cudaMemcpyAsync(v, e->volt.p, 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read volt");
+        if (c) ck(cudaMemcpyAsync(c, e->curr.p, 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read curr");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+efs_status efs_set_fields(efs_engine* e, const float* v, const float* c) {
+    return guard(e, [&] {
+        e->need_init();
+        if (v) ck(cudaMemcpyAsync(e->volt.p, v, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write volt");
+        if (c) ck(cudaMemcpyAsync(e->curr.p, c, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write curr");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+// state blob: magic, version, numTS, nbuf, then per buffer (bytes, data)
+static std::vector<DevBuf*> state_buffers(efs_engine* e) {
+    std::vector<DevBuf*> b = {&e->volt, &e->curr};
+    for (auto& r : e->pml) { b.push_back(&r->vflux); b.push_back(&r->cflux); }
+    if (e->mur_on) b.push_back(&e->mur_saved);
+    for (auto* s : {&e->ade_v, &e->ade_c}) if (s->n) { b.push_back(&s->state); b.push_back(&s->lor); }
+    if (e->rlc_on) { b.push_back(&e->rlc_vdn); b.push_back(&e->rlc_jn); b.push_back(&e->rlc_vil); }
+    if (e->ss_on) { b.push_back(&e->ss_e1); b.push_back(&e->ss_e2); }
+    if (e->pbc_on) b.push_back(&e->pbc_imag);
+    if (e->ring_on) b.push_back(&e->ring);
+    if (e->nf_on) { b.push_back(&e->nf_E); b.push_back(&e->nf_H); }
+    return b;
+}
+
+efs_status efs_get_state(efs_engine* e, void* buf, size_t cap, size_t* size) {
+    return guard(e, [&] {
+        e->need_init();
+        auto bufs = state_buffers(e);
+        size_t total = 4 * sizeof(uint64_t);
+        for (auto* d : bufs) total += sizeof(uint64_t) + d->bytes;
+        if (size) *size = total;
+        if (!buf) return;
+        if (cap < total) fail(EFS_ERR_INVALID, "state buffer too small");
+        uint8_t* p = static_cast<uint8_t*>(buf);
+        uint64_t hdr[4] = {0x45465342u /* "EFSB" */, 1, e->numTS, bufs.size()};
+        memcpy(p, hdr, sizeof(hdr));
+        p += sizeof(hdr);
+        for (auto* d : bufs) {
+            uint64_t nb = d->bytes;
+            memcpy(p, &nb, 8);
+            p += 8;
+            ck(cudaMemcpyAsync(p, d->p, d->bytes, cudaMemcpyDeviceToHost, e->stream), "state read");
+            p += d->bytes;
+        }
+        ck(cudaStreamSynchronize(e->stream), "sync");
+    });
+}
+
+efs_status efs_set_state(efs_engine* e, const void* buf, size_t size) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!buf || size < 4 * sizeof(uint64_t)) fail(EFS_ERR_INVALID, "state blob too small");
+        const uint8_t* p = static_cast<const uint8_t*>(buf);
+        uint64_t hdr[4];
+        memcpy(hdr, p, sizeof(hdr));
+        p += sizeof(hdr);
+        auto bufs = state_buffers(e);
+        if (hdr[0] != 0x45465342u || hdr[1] != 1 || hdr[3] != bufs.size()) fail(EFS_ERR_INVALID, "state blob does not match this engine's configuration");
+        const uint8_t* end = static_cast<const uint8_t*>(buf) + size;
+        for (auto* d : bufs) {
+            uint64_t nb;
+            if (p + 8 > end) fail(EFS_ERR_INVALID, "state blob truncated");
+            memcpy(&nb, p, 8);
+            p += 8;
+            if (nb != d->bytes || p + nb > end) fail(EFS_ERR_INVALID, "state blob buffer size mismatch");
+            ck(cudaMemcpyAsync(d->p, p, nb, cudaMemcpyHostToDevice, e->stream), "state write");
+            p += nb;
+        }
+        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->numTS = (uint32_t)hdr[2];
+        e->sync_state_to_device();
+    });
+}
+
+efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* out, size_t cap, size_t* count) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!name) fail(EFS_ERR_INVALID, "name must be non-null");
+        std::string s(name);
+        const DevBuf* b = nullptr;
+        size_t n = 0;
+        if ((s == "pml_volt_flux" || s == "pml_curr_flux") && arg < e->pml.size()) {
+            b = s == "pml_volt_flux" ? &e->pml[arg]->vflux : &e->pml[arg]->cflux;
+            n = e->pml[arg]->total;
+        } else if (s == "mur_saved" && e->mur_on) { b = &e->mur_saved; n = e->mur_n; }
+        else if (s == "ade_volt") { b = &e->ade_v.state; n = e->ade_v.n; }
+        else if (s == "ade_volt_lor") { b = &e->ade_v.lor; n = e->ade_v.n; }
+        else if (s == "ade_curr") { b = &e->ade_c.state; n = e->ade_c.n; }
+        else if (s == "ade_curr_lor") { b = &e->ade_c.lor; n = e->ade_c.n; }
+        else if (s == "rlc_vdn" && e->rlc_on) { b = &e->rlc_vdn; n = 3 * (size_t)e->rlc_n; }
+        else if (s == "rlc_jn" && e->rlc_on) { b = &e->rlc_jn; n = 3 * (size_t)e->rlc_n; }
+        else if (s == "rlc_vil" && e->rlc_on) { b = &e->rlc_vil; n = e->rlc_n; }
+        else if (s == "pbc_imag" && e->pbc_on) { b = &e->pbc_imag; n = e->pbc_imag.bytes / 4; }
+        else fail(EFS_ERR_INVALID, "unknown or unconfigured state name: " + s);
+        if (count) *count = n;
+        if (!out) return;
+        if (cap < n) fail(EFS_ERR_INVALID, "output buffer too small");
+        std::vector<float> tmp(n);
+        if (n) ck(cudaMemcpyAsync(tmp.data(), b->p, n * 4, cudaMemcpyDeviceToHost, e->stream), "debug read");
+        ck(cudaStreamSynchronize(e->stream), "sync");
+        if (s.rfind("rlc_", 0) == 0) {
+            // device keeps elements grouped by field cell; restore caller order
+            const size_t w = (s == "rlc_vil") ? 1 : 3;
+            for (size_t i = 0; i < e->rlc_n; ++i)
+                for (size_t q = 0; q < w; ++q) out[e->rlc_perm[i] * w + q] = tmp[i * w + q];
+        } else {
+            memcpy(out, tmp.data(), n * 4);
+        }
+    });
+}
+
+efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!ms || reps == 0) fail(EFS_ERR_INVALID, "ms must be non-null and reps > 0");
+        e->build_plan();
+        const Grid g = e->grid();
+        const PmlSet ps = e->pml_set();
+        const bool hp = !e->pml.empty();
+        dim3 cb(CORE_BZ, CORE_BY), cg(blocks(e->Nz, CORE_BZ), blocks(e->Ny, CORE_BY), blocks(e->Nx, CORE_TX));
+        cudaEvent_t ev[3];
+        for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+        auto volt = [&] {
+            if (e->indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, e->stream>>>(g, ps); }
+            else { if (hp) k_volt<false, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, e->stream>>>(g, ps); }
+        };
+        auto curr = [&] {
+            if (e->indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, e->stream>>>(g, ps); }
+            else { if (hp) k_curr<false, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_curr<false, false><<<cg, cb, 0, e->stream>>>(g, ps); }
+        };
+        ck(cudaEventRecord(ev[0], e->stream), "record");
+        for (uint32_t i = 0; i < reps; ++i) volt();
+        ck(cudaEventRecord(ev[1], e->stream), "record");
+        for (uint32_t i = 0; i < reps; ++i) curr();
+        ck(cudaEventRecord(ev[2], e->stream), "record");
+        ck(cudaEventSynchronize(ev[2]), "sync");
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        for (auto& x : ev) cudaEventDestroy(x);
+        ms[0] = a / reps;
+        ms[1] = b / reps;
+    });
+}
+
+efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
+        uint32_t k = 2;                                        // core E and H
+        k += e->ss_on + (e->ade_v.n > 0) + (e->ade_c.n > 0) + 3 * e->mur_on + 2 * e->rlc_on;
+        k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
+        k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;
+        k += e->nf_on + e->ring_on;
+        *out = k;
+    });
+}
+
+efs_status efs_device_bytes(const efs_engine* e, size_t* out) {
+    if (!e || !out) return EFS_ERR_INVALID;
+    size_t t = 0;
+    const DevBuf* all[] = {&e->volt, &e->curr, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
+    for (auto* b : all) t += b->bytes;
+    for (auto& r : e->pml) {
+        const DevBuf* rb[] = {&r->vv, &r->vvfo, &r->vvfn, &r->ii, &r->iifo, &r->iifn, &r->vflux, &r->cflux};
+        for (auto* b : rb) t += b->bytes;
+    }
+    t += e->nf_E.bytes + e->nf_H.bytes + e->ring.bytes;
+    *out = t;
+    return EFS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,672 @@
+// efs_kernels.cuh — device code of the B200 FDTD engine.
+//
+// Arithmetic: every field update is written with __fmul_rn/__fadd_rn/__fsub_rn
+// in the operand order of the reference's update expressions
+// (src/webgpu-engine.mjs WGSL, src/webgpu-fdtd.mjs CPU engine), so no FMA
+// contraction changes a result: the engine agrees bit for bit with an f32
+// restatement of the reference evaluated in the same order.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace efs {
+
+constexpr int MAX_PML = 24;     // UPML regions handled by the fused update
+constexpr int CORE_TX = 16;     // x-planes streamed per thread in the core kernels
+constexpr int CORE_BZ = 32;     // threads along z (contiguous axis)
+constexpr int CORE_BY = 8;      // threads along y
+
+struct StepState {              // device-resident, read by every per-step kernel
+    uint32_t numTS;
+    uint32_t ss_recording;
+    uint32_t ss_start;          // numTS at which steady-state recording began
+    uint32_t ss_base;           // sample count accumulated before ss_start
+};
+
+struct PmlRegion {
+    uint32_t s[3], n[3];
+    const float* vv; const float* vvfo; const float* vvfn;
+    const float* ii; const float* iifo; const float* iifn;
+    float* vflux; float* cflux;
+};
+struct PmlSet {
+    int count;
+    PmlRegion r[MAX_PML];
+};
+
+struct Grid {
+    uint32_t Nx, Ny, Nz, indexed;
+    size_t N, NyNz;
+    float* volt;
+    float* curr;
+    const uint32_t* mat;        // indexed mode: row per cell
+    const float* table;         //   12 floats per row
+    const float* vv; const float* vi; const float* ii; const float* iv;  // dense mode
+};
+
+__device__ __forceinline__ float upd(float vold, float cv, float ci, float curl) {
+    // V <- (V*vv) + vi*curl, each product rounded (src/webgpu-fdtd.mjs:76-82)
+    return __fadd_rn(__fmul_rn(vold, cv), __fmul_rn(ci, curl));
+}
+__device__ __forceinline__ float curl4(float a, float b, float c, float d) {
+    return __fadd_rn(__fsub_rn(__fsub_rn(a, b), c), d);
+}
+
+__device__ __forceinline__ bool in_region(const PmlRegion& r, uint32_t x, uint32_t y, uint32_t z) {
+    return (x - r.s[0]) < r.n[0] && (y - r.s[1]) < r.n[1] && (z - r.s[2]) < r.n[2];
+}
+__device__ __forceinline__ size_t region_p(const PmlRegion& r, uint32_t n, uint32_t x, uint32_t y, uint32_t z) {
+    size_t nyz = (size_t)r.n[1] * r.n[2];
+    return (size_t)n * r.n[0] * nyz + (size_t)(x - r.s[0]) * nyz + (size_t)(y - r.s[1]) * r.n[2] + (z - r.s[2]);
+}
+
+// One component of one cell through UPML pre -> core -> post
+// (src/webgpu-fdtd.mjs:239-358 around :1138/:1162).  `core` false: the core
+// update skips this cell (current loop bounds) but UPML still swaps.
+template <bool VOLT>
+__device__ __forceinline__ float pml_chain(const PmlSet& ps, uint32_t x, uint32_t y, uint32_t z, uint32_t n,
+                                           float vold, bool core, float cv, float ci, float curl) {
+    int cnt = 0, only = -1;
+    for (int r = 0; r < ps.count; ++r)
+        if (in_region(ps.r[r], x, y, z)) { ++cnt; only = r; }
+    if (cnt == 0) return core ? upd(vold, cv, ci, curl) : vold;
+    if (cnt == 1) {
+        const PmlRegion& R = ps.r[only];
+        size_t p = region_p(R, n, x, y, z);
+        float* flux = VOLT ? R.vflux : R.cflux;
+        const float a = VOLT ? R.vv[p] : R.ii[p];
+        const float b = VOLT ? R.vvfo[p] : R.iifo[p];
+        const float fn = VOLT ? R.vvfn[p] : R.iifn[p];
+        float fo = flux[p];
+        float fh = __fsub_rn(__fmul_rn(a, vold), __fmul_rn(b, fo));   // pre f_help
+        float v = core ? upd(fo, cv, ci, curl) : fo;                  // V = old flux, then core
+        flux[p] = v;                                                   // post: flux = V
+        return __fadd_rn(fh, __fmul_rn(fn, v));                        // V = f_help + fn*flux
+    }
+    // overlapping regions: the literal region-ordered sequence through memory
+    float v = vold;
+    for (int r = 0; r < ps.count; ++r) {
+        const PmlRegion& R = ps.r[r];
+        if (!in_region(R, x, y, z)) continue;
+        size_t p = region_p(R, n, x, y, z);
+        float* flux = VOLT ? R.vflux : R.cflux;
+        float a = VOLT ? R.vv[p] : R.ii[p], b = VOLT ? R.vvfo[p] : R.iifo[p];
+        float fo = flux[p];
+        float fh = __fsub_rn(__fmul_rn(a, v), __fmul_rn(b, fo));
+        v = fo;
+        flux[p] = fh;
+    }
+    if (core) v = upd(v, cv, ci, curl);
+    for (int r = 0; r < ps.count; ++r) {
+        const PmlRegion& R = ps.r[r];
+        if (!in_region(R, x, y, z)) continue;
+        size_t p = region_p(R, n, x, y, z);
+        float* flux = VOLT ? R.vflux : R.cflux;
+        float fn = VOLT ? R.vvfn[p] : R.iifn[p];
+        float fh = flux[p];
+        flux[p] = v;
+        v = __fadd_rn(fh, __fmul_rn(fn, v));
+    }
+    return v;
+}
+
+template <bool IDX>
+__device__ __forceinline__ void coeffs(const Grid& g, size_t c, int base, float out[6]) {
+    if (IDX) {
+        const float* t = g.table + (size_t)__ldg(g.mat + c) * 12 + base;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) out[k] = __ldg(t + k);
+    } else {
+        const float* a = base == 0 ? g.vv : g.ii;
+        const float* b = base == 0 ? g.vi : g.iv;
+        out[0] = __ldg(a + c); out[1] = __ldg(a + g.N + c); out[2] = __ldg(a + 2 * g.N + c);
+        out[3] = __ldg(b + c); out[4] = __ldg(b + g.N + c); out[5] = __ldg(b + 2 * g.N + c);
+    }
+}
+
+// E update (src/webgpu-engine.mjs:22-62 / src/webgpu-fdtd.mjs:64-106) with
+// UPML fused per cell.  Thread = one (y,z) column over CORE_TX x-planes;
+// Hy,Hz of plane x-1 stay in registers.
+template <bool IDX, bool PML>
+__global__ void __launch_bounds__(256) k_volt(const Grid g, const PmlSet ps) {
+    const uint32_t z = blockIdx.x * CORE_BZ + threadIdx.x;
+    const uint32_t y = blockIdx.y * CORE_BY + threadIdx.y;
+    if (z >= g.Nz || y >= g.Ny) return;
+    const uint32_t x0 = blockIdx.z * CORE_TX;
+    const uint32_t x1 = min(x0 + CORE_TX, g.Nx);
+    const size_t N = g.N, NyNz = g.NyNz;
+    const size_t sy = y > 0 ? g.Nz : 0, sz = z > 0 ? 1 : 0;
+    const float* __restrict__ H = g.curr;
+    float* __restrict__ V = g.volt;
+    size_t c = (size_t)x0 * NyNz + (size_t)y * g.Nz + z;
+    float hy_p, hz_p;
+    if (x0 > 0) { hy_p = __ldg(H + N + c - NyNz); hz_p = __ldg(H + 2 * N + c - NyNz); }
+    else { hy_p = __ldg(H + N + c); hz_p = __ldg(H + 2 * N + c); }
+    for (uint32_t x = x0; x < x1; ++x, c += NyNz) {
+        const float hx = __ldg(H + c), hy = __ldg(H + N + c), hz = __ldg(H + 2 * N + c);
+        const float hz_ym = __ldg(H + 2 * N + c - sy), hy_zm = __ldg(H + N + c - sz);
+        const float hx_zm = __ldg(H + c - sz), hx_ym = __ldg(H + c - sy);
+        const float cx = curl4(hz, hz_ym, hy, hy_zm);
+        const float cy = curl4(hx, hx_zm, hz, hz_p);
+        const float cz = curl4(hy, hy_p, hx, hx_ym);
+        float k[6];
+        coeffs<IDX>(g, c, 0, k);
+        const float e0 = V[c], e1 = V[N + c], e2 = V[2 * N + c];
+        if (PML) {
+            V[c] = pml_chain<true>(ps, x, y, z, 0, e0, true, k[0], k[3], cx);
+            V[N + c] = pml_chain<true>(ps, x, y, z, 1, e1, true, k[1], k[4], cy);
+            V[2 * N + c] = pml_chain<true>(ps, x, y, z, 2, e2, true, k[2], k[5], cz);
+        } else {
+            V[c] = upd(e0, k[0], k[3], cx);
+            V[N + c] = upd(e1, k[1], k[4], cy);
+            V[2 * N + c] = upd(e2, k[2], k[5], cz);
+        }
+        hy_p = hy; hz_p = hz;
+    }
+}
+
+// H update (src/webgpu-engine.mjs:80-121 / src/webgpu-fdtd.mjs:113-155):
+// core over (Nx-1)(Ny-1)(Nz-1), UPML over every region cell.
+template <bool IDX, bool PML>
+__global__ void __launch_bounds__(256) k_curr(const Grid g, const PmlSet ps) {
+    const uint32_t z = blockIdx.x * CORE_BZ + threadIdx.x;
+    const uint32_t y = blockIdx.y * CORE_BY + threadIdx.y;
+    if (z >= g.Nz || y >= g.Ny) return;
+    const uint32_t x0 = blockIdx.z * CORE_TX;
+    const uint32_t x1 = min(x0 + CORE_TX, g.Nx);
+    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
+    const bool yz_core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
+    if (!PML && !yz_core) return;
+    const float* __restrict__ V = g.volt;
+    float* __restrict__ H = g.curr;
+    size_t c = (size_t)x0 * NyNz + (size_t)y * Nz + z;
+    float ey_c = 0.f, ez_c = 0.f;
+    if (yz_core) { ey_c = __ldg(V + N + c); ez_c = __ldg(V + 2 * N + c); }
+    for (uint32_t x = x0; x < x1; ++x, c += NyNz) {
+        const bool core = yz_core && (x + 1 < g.Nx);
+        float cx = 0.f, cy = 0.f, cz = 0.f;
+        if (core) {
+            const float ex = __ldg(V + c);
+            const float ez_yp = __ldg(V + 2 * N + c + Nz), ey_zp = __ldg(V + N + c + 1);
+            const float ex_zp = __ldg(V + c + 1), ex_yp = __ldg(V + c + Nz);
+            const float ey_xp = __ldg(V + N + c + NyNz), ez_xp = __ldg(V + 2 * N + c + NyNz);
+            cx = curl4(ez_c, ez_yp, ey_c, ey_zp);
+            cy = curl4(ex, ex_zp, ez_c, ez_xp);
+            cz = curl4(ey_c, ey_xp, ex, ex_yp);
+            ey_c = ey_xp; ez_c = ez_xp;
+        }
+        if (PML) {
+            float k[6] = {0, 0, 0, 0, 0, 0};
+            if (core) coeffs<IDX>(g, c, 6, k);
+            const float h0 = H[c], h1 = H[N + c], h2 = H[2 * N + c];
+            const float r0 = pml_chain<false>(ps, x, y, z, 0, h0, core, k[0], k[3], cx);
+            const float r1 = pml_chain<false>(ps, x, y, z, 1, h1, core, k[1], k[4], cy);
+            const float r2 = pml_chain<false>(ps, x, y, z, 2, h2, core, k[2], k[5], cz);
+            if (core || r0 != h0 || r1 != h1 || r2 != h2) { H[c] = r0; H[N + c] = r1; H[2 * N + c] = r2; }
+            // (bitwise-equal rewrites of untouched cells are skipped; NaN != NaN rewrites are harmless)
+        } else if (core) {
+            float k[6];
+            coeffs<IDX>(g, c, 6, k);
+            H[c] = upd(H[c], k[0], k[3], cx);
+            H[N + c] = upd(H[N + c], k[1], k[4], cy);
+            H[2 * N + c] = upd(H[2 * N + c], k[2], k[5], cz);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sparse per-step operations
+// ---------------------------------------------------------------------------
+
+// Additive point sources grouped by target so repeated targets keep the
+// reference's sequential order: group g covers entries [off[g], off[g+1]).
+// kind 0 = excitation (src/webgpu-fdtd.mjs:161-185, C++ past-end semantics)
+// kind 1 = TFSF (src/webgpu-fdtd.mjs:694-733, interpolated, skipped past end)
+struct PointSources {
+    uint32_t ngroups;
+    const uint32_t* target;     // field index per group
+    const uint32_t* off;        // ngroups+1
+    const uint32_t* delay;      // per entry
+    const float* amp;           // per entry
+    const float* frac;          // per entry (TFSF)
+    const float* signal;
+    uint32_t len, period;
+};
+
+template <int KIND>
+__global__ void k_point_sources(float* __restrict__ F, const StepState* st, uint32_t k, const PointSources s) {
+    uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= s.ngroups) return;
+    const int64_t ts = (int64_t)st->numTS + k;
+    const uint32_t t = s.target[gi];
+    float v = F[t];
+    for (uint32_t e = s.off[gi]; e < s.off[gi + 1]; ++e) {
+        if (KIND == 0) {
+            int64_t p = s.period > 0 ? (int64_t)s.period : ts + 1;
+            int64_t pos = ts - (int64_t)s.delay[e];
+            if (pos < 0) pos = 0;
+            pos %= p;
+            if (pos >= (int64_t)s.len) pos = 0;
+            v = __fadd_rn(v, __fmul_rn(s.amp[e], s.signal[pos]));
+        } else {
+            int64_t d = ts - (int64_t)s.delay[e];
+            if (d < 0) continue;
+            if (s.period > 0) d %= (int64_t)s.period;
+            if (d >= (int64_t)s.len - 1) continue;
+            const float delta = s.frac[e];
+            const float sig = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, delta), s.signal[d]), __fmul_rn(delta, s.signal[d + 1]));
+            v = __fadd_rn(v, __fmul_rn(s.amp[e], sig));
+        }
+    }
+    F[t] = v;
+}
+
+// A field read that the reference makes after the UPML pre-update: for a cell
+// inside a region the value there is the region's old flux.  sel 0 = field,
+// sel r+1 = flux of region r.
+struct ReadLoc { uint32_t sel, idx; };
+
+__device__ __forceinline__ float read_loc(const float* F, const float* const* flux, ReadLoc l) {
+    return l.sel == 0 ? F[l.idx] : flux[l.sel - 1][l.idx];
+}
+
+// Mur ABC (src/webgpu-fdtd.mjs:992-1023)
+struct MurDev {
+    uint32_t n, napply;
+    const float* coeff;
+    const ReadLoc* pre_normal;     // reads after the UPML pre swap
+    const ReadLoc* pre_shifted;
+    const uint32_t* shifted;
+    const uint32_t* apply_target;  // unique normal indices
+    const uint32_t* apply_src;     // last entry that writes each target
+    float* saved;
+    const float* const* vflux;
+};
+__global__ void k_mur_pre(const float* __restrict__ V, const MurDev m) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    float s = read_loc(V, m.vflux, m.pre_shifted[i]);
+    float nv = read_loc(V, m.vflux, m.pre_normal[i]);
+    m.saved[i] = __fsub_rn(s, __fmul_rn(m.coeff[i], nv));
+}
+__global__ void k_mur_post(const float* __restrict__ V, const MurDev m) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    m.saved[i] = __fadd_rn(m.saved[i], __fmul_rn(m.coeff[i], V[m.shifted[i]]));
+}
+__global__ void k_mur_apply(float* __restrict__ V, const MurDev m) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.napply) return;
+    V[m.apply_target[i]] = m.saved[m.apply_src[i]];
+}
+
+// Lorentz/Drude ADE state update (src/webgpu-fdtd.mjs:405-454), all orders
+// and directions of one field flattened into one list.
+struct AdeDev {
+    uint32_t n;
+    const ReadLoc* src;
+    const uint8_t* lorentz;
+    const float* kint; const float* kext; const float* klor;
+    float* state; float* lor;
+    const float* const* flux;
+};
+__global__ void k_ade(const float* __restrict__ F, const AdeDev a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float v = read_loc(F, a.flux, a.src[i]);
+    const float st = a.state[i];
+    if (a.lorentz[i]) {
+        const float l = __fadd_rn(a.lor[i], __fmul_rn(a.klor[i], st));
+        a.lor[i] = l;
+        a.state[i] = __fadd_rn(__fmul_rn(a.kint[i], st), __fmul_rn(a.kext[i], __fsub_rn(v, l)));
+    } else {
+        a.state[i] = __fadd_rn(__fmul_rn(a.kint[i], st), __fmul_rn(a.kext[i], v));
+    }
+}
+
+// Lumped RLC (src/webgpu-fdtd.mjs:775-863, CPU order: pre before the core E
+// update, apply after Mur apply).  Elements sharing a field cell are grouped.
+struct RlcDev {
+    uint32_t n, ngroups;
+    const uint32_t* gtarget; const uint32_t* goff;  // groups over element ids
+    const uint32_t* type;
+    const float* p;        // 9 per element: i2v ilv vvd vv2 vj1 vj2 ib0 b1 b2
+    float* vdn; float* jn; float* vil;
+};
+__global__ void k_rlc_pre(const RlcDev r) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= r.n) return;
+    float* V = r.vdn + 3 * (size_t)i;
+    V[2] = V[1];
+    V[1] = V[0];
+    if (r.type[i] == 0) {
+        const float* p = r.p + 9 * (size_t)i;
+        r.vil[i] = __fadd_rn(r.vil[i], __fmul_rn(__fmul_rn(p[0], p[1]), V[1]));
+    }
+}
+__global__ void k_rlc_apply(float* __restrict__ F, const RlcDev r) {
+    uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= r.ngroups) return;
+    const uint32_t g = r.gtarget[gi];
+    for (uint32_t e = r.goff[gi]; e < r.goff[gi + 1]; ++e) {
+        float* V = r.vdn + 3 * (size_t)e;
+        float* J = r.jn + 3 * (size_t)e;
+        V[0] = F[g];
+        J[2] = J[1];
+        J[1] = J[0];
+        if (r.type[e] == 1) {
+            const float* p = r.p + 9 * (size_t)e;  // p: i2v ilv vvd vv2 vj1 vj2 ib0 b1 b2
+            float in = __fsub_rn(V[0], r.vil[e]);
+            in = __fadd_rn(in, __fmul_rn(p[3], V[2]));
+            in = __fadd_rn(in, __fmul_rn(p[4], J[1]));
+            in = __fadd_rn(in, __fmul_rn(p[5], J[2]));
+            const float v0 = __fmul_rn(p[2], in);
+            V[0] = v0;
+            float j = __fmul_rn(p[6], __fsub_rn(v0, V[2]));
+            j = __fsub_rn(j, __fmul_rn(__fmul_rn(p[7], p[6]), J[1]));
+            j = __fsub_rn(j, __fmul_rn(__fmul_rn(p[8], p[6]), J[2]));
+            J[0] = j;
+            F[g] = v0;
+        }
+    }
+}
+
+// Steady-state energy accumulation (src/webgpu-fdtd.mjs:1054-1070); the
+// sample counter is derived from numTS so the kernel needs no atomics.
+__global__ void k_steady_state(const float* __restrict__ V, const StepState* st, uint32_t k, const uint32_t* idx,
+                               uint32_t n, uint32_t period, float* e1, float* e2) {
+    if (!st->ss_recording) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t sample = st->ss_base + (st->numTS + k - st->ss_start);
+    const float v = V[idx[i]];
+    const float e = __fmul_rn(v, v);
+    if (sample < period) e1[i] = __fadd_rn(e1[i], e);
+    else e2[i] = __fadd_rn(e2[i], e);
+}
+
+// Periodic / Bloch copy (src/webgpu-engine.mjs:519-584), one axis per launch.
+struct PbcDev {
+    uint32_t axis, volt, src, dst, fs0, fs1, b0, b1;
+    uint32_t Nx, Ny, Nz;
+    float cosP, sinP;
+    float* imag;       // Bloch imaginary parts of this axis, already offset
+};
+__global__ void k_pbc(float* __restrict__ F, const PbcDev p) {
+    const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i1 = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i0 >= p.b0 || i1 >= p.b1) return;
+    const uint32_t t0 = (p.axis + 1) % 3, t1 = (p.axis + 2) % 3;
+    uint32_t sp[3], dp[3];
+    if (p.axis == 0) { sp[0] = p.src; sp[1] = i0; sp[2] = i1; dp[0] = p.dst; dp[1] = i0; dp[2] = i1; }
+    else if (p.axis == 1) { sp[0] = i1; sp[1] = p.src; sp[2] = i0; dp[0] = i1; dp[1] = p.dst; dp[2] = i0; }
+    else { sp[0] = i0; sp[1] = i1; sp[2] = p.src; dp[0] = i0; dp[1] = i1; dp[2] = p.dst; }
+    const size_t N = (size_t)p.Nx * p.Ny * p.Nz, NyNz = (size_t)p.Ny * p.Nz;
+    const size_t s = (size_t)sp[0] * NyNz + (size_t)sp[1] * p.Nz + sp[2];
+    const size_t d = (size_t)dp[0] * NyNz + (size_t)dp[1] * p.Nz + dp[2];
+    const size_t s0 = t0 * N + s, d0 = t0 * N + d, s1 = t1 * N + s, d1 = t1 * N + d;
+    if (p.sinP == 0.0f) {
+        F[d0] = __fmul_rn(p.cosP, F[s0]);
+        F[d1] = __fmul_rn(p.cosP, F[s1]);
+    } else {
+        const size_t fl = (size_t)i0 * p.fs1 + i1, face = (size_t)p.fs0 * p.fs1;
+        float* im = p.imag + (p.volt ? 0 : 2 * face);
+        float r0 = F[s0], q0 = im[fl];
+        F[d0] = __fsub_rn(__fmul_rn(p.cosP, r0), __fmul_rn(p.sinP, q0));
+        im[fl] = __fadd_rn(__fmul_rn(p.sinP, r0), __fmul_rn(p.cosP, q0));
+        float r1 = F[s1], q1 = im[face + fl];
+        F[d1] = __fsub_rn(__fmul_rn(p.cosP, r1), __fmul_rn(p.sinP, q1));
+        im[face + fl] = __fadd_rn(__fmul_rn(p.sinP, r1), __fmul_rn(p.cosP, q1));
+    }
+}
+
+// Probe gather (src/webgpu-engine.mjs:2593-2606 direct, :2644-2665 ring).
+// Ring row = sample index derived from numTS: rows are written at
+// (numTS+1) % interval == 0, counted from configure time.
+__global__ void k_gather_ring(const float* __restrict__ V, const float* __restrict__ C, const StepState* st, uint32_t k,
+                              const uint32_t* idx, uint32_t G, uint32_t interval, uint32_t q0, uint32_t maxS, float* ring) {
+    const uint32_t ts1 = st->numTS + k + 1;
+    if (ts1 % interval != 0) return;
+    const uint32_t q = ts1 / interval;
+    if (q <= q0) return;
+    const uint32_t s = q - 1 - q0;
+    if (s >= maxS) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    const uint32_t t = idx[i];
+    float* row = ring + (size_t)s * G * 2;
+    row[2 * i] = V[t];
+    row[2 * i + 1] = C[t];
+}
+__global__ void k_gather(const float* __restrict__ V, const float* __restrict__ C, const uint32_t* idx, uint32_t G, float* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    out[2 * i] = V[idx[i]];
+    out[2 * i + 1] = C[idx[i]];
+}
+
+__global__ void k_advance(StepState* st, uint32_t n) { st->numTS += n; }
+
+// ---------------------------------------------------------------------------
+// NF2FF running DFT (src/webgpu-engine.mjs:675-799) for F frequencies.  The
+// phase omega*dT*n is formed in f64 and reduced modulo 2*pi before the
+// cosine/sine (the reference forms it in f32, :777-782, which loses digits
+// as n grows); the accumulation stays f32 in the reference's operand order.
+// ---------------------------------------------------------------------------
+constexpr int NF_MAX_FREQ = 16;
+struct Nf2ffDev {
+    uint32_t np, nf, maxTS, window;
+    uint32_t Nx, Ny, Nz;
+    uint32_t off[6];
+    const uint32_t* pts;
+    const float* el;
+    float* accE; float* accH;       // [f][pid*6+k]
+    double wdt[NF_MAX_FREQ];        // omega*dT per frequency (f64)
+    float dT32, wnorm;
+};
+__global__ void __launch_bounds__(256) k_nf2ff(const float* __restrict__ V, const float* __restrict__ C, const StepState* st,
+                                               uint32_t k, const Nf2ffDev d) {
+    __shared__ float tw[NF_MAX_FREQ][4];
+    __shared__ float s_wdt;
+    const uint32_t ts = st->numTS + k + 1;     // WebGPUEngine.iterate passes numTS+1 (:2484)
+    if (threadIdx.x < d.nf) {
+        const double two_pi = 6.283185307179586476925286766559;
+        const double pe = fmod(d.wdt[threadIdx.x] * (double)ts, two_pi);
+        const double ph = fmod(d.wdt[threadIdx.x] * ((double)ts + 0.5), two_pi);
+        double s, c;
+        sincos(pe, &s, &c);
+        tw[threadIdx.x][0] = (float)c; tw[threadIdx.x][1] = (float)s;
+        sincos(ph, &s, &c);
+        tw[threadIdx.x][2] = (float)c; tw[threadIdx.x][3] = (float)s;
+    }
+    if (threadIdx.x == 0) {
+        float ww = 1.0f;
+        if (d.window == 1 && d.maxTS > 1) {
+            const double two_pi = 6.283185307179586476925286766559;
+            ww = (float)(0.5 * (1.0 - cos(two_pi * (double)ts / (double)(d.maxTS - 1))));
+        }
+        s_wdt = __fmul_rn(__fmul_rn(ww, d.wnorm), d.dT32);
+    }
+    __syncthreads();
+    const uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= d.np) return;
+    const uint32_t ix = d.pts[3 * pid], iy = d.pts[3 * pid + 1], iz = d.pts[3 * pid + 2];
+    const size_t Ny = d.Ny, Nz = d.Nz, N = (size_t)d.Nx * Ny * Nz, NyNz = Ny * Nz;
+    auto fi = [&](uint32_t x, uint32_t y, uint32_t z) { return (size_t)x * NyNz + (size_t)y * Nz + z; };
+    const size_t base = fi(ix, iy, iz);
+    const bool atB = (ix >= d.Nx - 1) || (iy >= d.Ny - 1) || (iz >= d.Nz - 1);
+    float E[3] = {0.f, 0.f, 0.f}, Hh[3] = {0.f, 0.f, 0.f};
+    if (!atB) {
+        const float elX = d.el[d.off[0] + ix], elY = d.el[d.off[1] + iy], elZ = d.el[d.off[2] + iz];
+        float a = __fadd_rn(__fadd_rn(__fadd_rn(V[base], V[fi(ix, iy + 1, iz)]), V[fi(ix, iy + 1, iz + 1)]), V[fi(ix, iy, iz + 1)]);
+        E[0] = __fdiv_rn(a, __fmul_rn(4.0f, elX));
+        a = __fadd_rn(__fadd_rn(__fadd_rn(V[N + base], V[N + fi(ix, iy, iz + 1)]), V[N + fi(ix + 1, iy, iz + 1)]), V[N + fi(ix + 1, iy, iz)]);
+        E[1] = __fdiv_rn(a, __fmul_rn(4.0f, elY));
+        a = __fadd_rn(__fadd_rn(__fadd_rn(V[2 * N + base], V[2 * N + fi(ix + 1, iy, iz)]), V[2 * N + fi(ix + 1, iy + 1, iz)]), V[2 * N + fi(ix, iy + 1, iz)]);
+        E[2] = __fdiv_rn(a, __fmul_rn(4.0f, elZ));
+    }
+    const uint32_t pos[3] = {ix, iy, iz}, lim[3] = {d.Nx, d.Ny, d.Nz};
+    const size_t step[3] = {NyNz, Nz, 1};
+    for (int n = 0; n < 3; ++n) {
+        const float d0 = d.el[d.off[3 + n] + pos[n]];
+        if (!(d0 > 0.0f)) continue;
+        float h = __fdiv_rn(C[n * N + base], d0);
+        if (pos[n] < lim[n] - 1) {
+            const float d1 = d.el[d.off[3 + n] + pos[n] + 1];
+            const float dr = __fdiv_rn(d0, __fadd_rn(d0, d1));
+            const float hu = __fdiv_rn(C[n * N + base + step[n]], d1);
+            h = __fadd_rn(__fmul_rn(h, __fsub_rn(1.0f, dr)), __fmul_rn(hu, dr));
+        }
+        Hh[n] = h;
+    }
+    const float w = s_wdt;
+    for (uint32_t f = 0; f < d.nf; ++f) {
+        float* aE = d.accE + ((size_t)f * d.np + pid) * 6;
+        float* aH = d.accH + ((size_t)f * d.np + pid) * 6;
+        const float ce = tw[f][0], se = -tw[f][1], ch = tw[f][2], sh = -tw[f][3];
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            aE[2 * n] = __fadd_rn(aE[2 * n], __fmul_rn(__fmul_rn(E[n], ce), w));
+            aE[2 * n + 1] = __fadd_rn(aE[2 * n + 1], __fmul_rn(__fmul_rn(E[n], se), w));
+            aH[2 * n] = __fadd_rn(aH[2 * n], __fmul_rn(__fmul_rn(Hh[n], ch), w));
+            aH[2 * n + 1] = __fadd_rn(aH[2 * n + 1], __fmul_rn(__fmul_rn(Hh[n], sh), w));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Energy: sum over interior cells of volt^2 + curr^2 (src/webgpu-engine.mjs:
+// 3071-3145), block-then-warp reduction with f64 block partials.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_energy(const float* __restrict__ V, const float* __restrict__ C, uint32_t Nx,
+                                                uint32_t Ny, uint32_t Nz, double* partial) {
+    const size_t N = (size_t)Nx * Ny * Nz, inner = (size_t)(Nx - 1) * (Ny - 1) * (Nz - 1);
+    const size_t iNz = Nz - 1, iNyNz = (size_t)(Ny - 1) * (Nz - 1);
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < inner; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t x = i / iNyNz, r = i - x * iNyNz, y = r / iNz, z = r - y * iNz;
+        const size_t c = x * Ny * Nz + y * Nz + z;
+        float s = 0.f;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            const float v = __ldg(V + n * N + c), h = __ldg(C + n * N + c);
+            s = __fadd_rn(__fadd_rn(s, __fmul_rn(v, v)), __fmul_rn(h, h));
+        }
+        acc += (double)s;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+__global__ void k_energy_final(const double* partial, uint32_t n, double* out) {
+    double acc = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) *out = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// NF2FF far field (src/webgpu-engine.mjs:830-985).  Thread = one (theta,phi)
+// angle; a block stages a tile of surface points in shared memory (surface
+// currents Js = n x H, Ms = -n x E precomputed per point) and every thread
+// sweeps the tile.  blockIdx.y splits the points so the grid fills the SMs;
+// k_far_field_final sums the chunks in f64 and forms E_theta, E_phi, P_rad.
+// ---------------------------------------------------------------------------
+constexpr int FF_THREADS = 256;
+constexpr int FF_TILE = 256;
+struct FarFieldDev {
+    uint32_t np, nth, nph, chunk;
+    float k, cx, cy, cz;
+    const float* accE; const float* accH; const float* meta;
+    const float* theta; const float* phi;
+    float* partial;          // [chunks][A][8]
+};
+__global__ void __launch_bounds__(FF_THREADS) k_far_field(const FarFieldDev d) {
+    __shared__ float sp[FF_TILE][16];   // pos xyz, area, J re/im xyz, M re/im xyz
+    const uint32_t A = d.nth * d.nph;
+    const uint32_t a = blockIdx.x * FF_THREADS + threadIdx.x;
+    const bool live = a < A;
+    float sT = 0, cT = 0, sP = 0, cP = 0;
+    if (live) {
+        const float th = d.theta[a / d.nph], ph = d.phi[a % d.nph];
+        sincosf(th, &sT, &cT);
+        sincosf(ph, &sP, &cP);
+    }
+    const float cTcP = cT * cP, cTsP = cT * sP, sTcP = sT * cP, sTsP = sT * sP;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint32_t p0 = blockIdx.y * d.chunk, p1 = min(p0 + d.chunk, d.np);
+    for (uint32_t t0 = p0; t0 < p1; t0 += FF_TILE) {
+        const uint32_t nt = min((uint32_t)FF_TILE, p1 - t0);
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nt; j += FF_THREADS) {
+            const uint32_t p = t0 + j;
+            const float* m = d.meta + 8 * (size_t)p;
+            const float* E = d.accE + 6 * (size_t)p;
+            const float* H = d.accH + 6 * (size_t)p;
+            const int nd = (int)m[3];
+            const float s = m[4];
+            float J[6] = {0, 0, 0, 0, 0, 0}, M[6] = {0, 0, 0, 0, 0, 0};   // [comp*2 + re/im]
+            for (int c = 0; c < 2; ++c) {
+                if (nd == 0) { J[2 + c] = -s * H[4 + c]; J[4 + c] = s * H[2 + c]; M[2 + c] = s * E[4 + c]; M[4 + c] = -s * E[2 + c]; }
+                else if (nd == 1) { J[0 + c] = s * H[4 + c]; J[4 + c] = -s * H[0 + c]; M[0 + c] = -s * E[4 + c]; M[4 + c] = s * E[0 + c]; }
+                else { J[0 + c] = -s * H[2 + c]; J[2 + c] = s * H[0 + c]; M[0 + c] = s * E[2 + c]; M[2 + c] = -s * E[0 + c]; }
+            }
+            sp[j][0] = m[0] - d.cx; sp[j][1] = m[1] - d.cy; sp[j][2] = m[2] - d.cz; sp[j][3] = m[5];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { sp[j][4 + q] = J[q]; sp[j][10 + q] = M[q]; }
+        }
+        __syncthreads();
+        if (live) {
+            for (uint32_t j = 0; j < nt; ++j) {
+                const float* q = sp[j];
+                const float rc = q[0] * sTcP + q[1] * sTsP + q[2] * cT;
+                float sn, cs;
+                sincosf(d.k * rc, &sn, &cs);
+                const float ar = q[3] * cs, ai = q[3] * sn;
+                const float Jtr = q[4] * cTcP + q[6] * cTsP - q[8] * sT, Jti = q[5] * cTcP + q[7] * cTsP - q[9] * sT;
+                const float Jpr = q[6] * cP - q[4] * sP, Jpi = q[7] * cP - q[5] * sP;
+                const float Mtr = q[10] * cTcP + q[12] * cTsP - q[14] * sT, Mti = q[11] * cTcP + q[13] * cTsP - q[15] * sT;
+                const float Mpr = q[12] * cP - q[10] * sP, Mpi = q[13] * cP - q[11] * sP;
+                acc[0] += ar * Jtr - ai * Jti; acc[1] += ar * Jti + ai * Jtr;
+                acc[2] += ar * Jpr - ai * Jpi; acc[3] += ar * Jpi + ai * Jpr;
+                acc[4] += ar * Mtr - ai * Mti; acc[5] += ar * Mti + ai * Mtr;
+                acc[6] += ar * Mpr - ai * Mpi; acc[7] += ar * Mpi + ai * Mpr;
+            }
+        }
+    }
+    if (live) {
+        float* o = d.partial + ((size_t)blockIdx.y * A + a) * 8;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) o[q] = acc[q];
+    }
+}
+__global__ void k_far_field_final(const float* partial, uint32_t A, uint32_t chunks, double fre, double fim, float* out) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A) return;
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t c = 0; c < chunks; ++c)
+        for (int q = 0; q < 8; ++q) s[q] += (double)partial[((size_t)c * A + a) * 8 + q];
+    const double Z0 = 376.73031346177066;
+    const double ar = s[6] + Z0 * s[0], ai = s[7] + Z0 * s[1];
+    const double Etr = -(fre * ar - fim * ai), Eti = -(fre * ai + fim * ar);
+    const double br = s[4] - Z0 * s[2], bi = s[5] - Z0 * s[3];
+    const double Epr = fre * br - fim * bi, Epi = fre * bi + fim * br;
+    float* o = out + 5 * (size_t)a;
+    o[0] = (float)((Etr * Etr + Eti * Eti + Epr * Epr + Epi * Epi) / (2 * Z0));
+    o[1] = (float)Etr; o[2] = (float)Eti; o[3] = (float)Epr; o[4] = (float)Epi;
+}
+
+}  // namespace efs

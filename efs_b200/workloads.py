@@ -1,0 +1,228 @@
+"""Jobs: the engine inputs of one solve, and the caller loop that drives them.
+
+A job is a dict holding exactly what the reference's orchestrator extracts
+from openEMS before it drives the engine (scripts/lib/sim-engine.mjs:533-638):
+grid, coefficients, excitation, UPML regions, Mur config, TFSF config,
+probes, NF2FF surface, dT, step budget and end criterion.  `configure`
+replays the orchestrator's configure* sequence on any engine with the
+WebGPUEngine method names (the CUDA engine, or the CPU oracle in tests), and
+`run` replays its stepping loop (iterate in batches of 100, lagged energy
+check, probe readback, :648-696).
+"""
+import math
+
+import numpy as np
+
+from . import opgen
+
+
+def openems_cavity():
+    """The native-openEMS engine_comparison cavity (reference
+    tests/generate_fixtures.py:439-500): 16x8x18 lines over 5x2x6 cm, PEC
+    walls, Gaussian f0 = 5.5 GHz / fc = 4.5 GHz on the staircase from node
+    (10,5,12) to (11,6,13), voltage probe on the z edge at (5,3,4) every 2
+    steps, 500 steps.  dT is the fixture's (half its 1.23293515115e-11 s
+    sample spacing)."""
+    def lin(a, b, n):
+        st = (b - a) / (n - 1)
+        return [float("%.10e" % (a + i * st)) for i in range(n)]   # as written to the XML
+    mesh = opgen.Mesh(lin(0, 5e-2, 16), lin(0, 2e-2, 8), lin(0, 6e-2, 18))
+    dT = 1.23293515115e-11 / 2
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT)
+    sig = opgen.gauss_signal(5.5e9, 4.5e9, dT, 500)
+    Nx, Ny, Nz = mesh.shape
+    p1 = [mesh.lines[k][i] for k, i in enumerate((10, 5, 12))]
+    p2 = [mesh.lines[k][i] for k, i in enumerate((11, 6, 13))]
+    amp, dirs, pos = [], [], []
+    for n, (x, y, z) in opgen.find_path(mesh, p1, p2):
+        amp.append(mesh.dl(n)[(x, y, z)[n]])
+        dirs.append(n)
+        pos.append(x * Ny * Nz + y * Nz + z)
+    probe = opgen.voltage_probe(mesh, [5, 3, 4], [5, 3, 5], 1.0, 2)
+    return dict(name="openems_cavity", grid=list(mesh.shape), dT=dT, maxTS=500, endCrit=0.0, mesh=mesh,
+                coefficients=dict(vv=opgen.flat(vv), vi=opgen.flat(vi), ii=opgen.flat(ii), iv=opgen.flat(iv)),
+                excitation=dict(signal=sig.astype(np.float32), delay=[0] * len(amp), amp=np.float32(amp), dir=dirs,
+                                pos=pos, period=0),
+                probes=[probe], include_t0=True)
+
+
+class _LazyCells:
+    """Per-cell property looked up from a uint8 material-id grid on slicing."""
+
+    def __init__(self, ids, values):
+        self.ids = ids
+        self.values = np.asarray(values, np.float64)
+
+    def __getitem__(self, sl):
+        return self.values[self.ids[sl]]
+
+
+def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_inset=20, nf2ff_inset=10,
+                steps=20000, f0=10e9, fc=5e9, chunk=32, tfsf=True, nf2ff=True):
+    """Plain large solve (the benchmark's headline workload at n = 512):
+    uniform n^3 lines with spacing delta; `nboxes` seeded axis-aligned boxes
+    (numpy default_rng(seed)), the first half PEC, the rest dielectric with
+    eps_r ~ U[2, 10]; Mur ABC on the x and y faces, `pml`-cell UPML on the z
+    faces; a TFSF Gaussian plane wave (f0, fc) at normal incidence along +z,
+    E along x, on the box `tfsf_inset` cells inside the boundary; NF2FF box
+    `nf2ff_inset` cells inside with `nfreq` frequencies spread over the pulse
+    band.  Coefficients come out as a material index + table."""
+    lines = opgen.uniform_lines(n, delta)
+    mesh = opgen.Mesh(lines, lines, lines)
+    dT = opgen.cfl_dt(mesh)
+    rng = np.random.default_rng(seed)
+    nc = n - 1
+    ids = np.zeros((nc, nc, nc), np.uint8)
+    eps_vals = [1.0]
+    pec_boxes = []
+    margin = tfsf_inset + 4
+    lo_cap = max(margin, 1)
+    for i in range(nboxes):
+        size = rng.integers(max(2, n // 32), max(3, n // 8), 3)
+        lo = np.array([rng.integers(lo_cap, max(lo_cap + 1, nc - margin - s)) for s in size])
+        hi = np.minimum(lo + size, nc - margin)
+        if i < nboxes // 2:
+            pec_boxes.append(([lines[lo[a]] for a in range(3)], [lines[hi[a]] for a in range(3)]))
+        else:
+            eps_vals.append(float(rng.uniform(2.0, 10.0)))
+            ids[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = len(eps_vals) - 1
+    eps = _LazyCells(ids, eps_vals)
+
+    def pec(nn, x0, x1):
+        m = np.zeros((x1 - x0, n, n), bool)
+        for lo, hi in pec_boxes:
+            m |= opgen.edge_mask_in_box(mesh, nn, lo, hi, xslice=slice(x0, x1))
+        return m
+    bc = (2, 2, 2, 2, 3, 3)
+    boxes = [((0, 0, 0), (n, n, pml)), ((0, 0, n - pml), (n, n, pml))] if pml else []
+    sig_fns = [None, None, opgen.pml_sigma(mesh, 2, pml, pml)] if pml else [None] * 3
+    mt = opgen.MaterialTable()
+    mat = np.empty(n * n * n, np.uint32)
+    for x0 in range(0, n, chunk):
+        x1 = min(n, x0 + chunk)
+        vv, vi, ii, iv = opgen.operator_dense(mesh, dT, eps_r=eps, pec_edges=pec, bc=bc, x0=x0, x1=x1)
+        if boxes:
+            opgen.upml_apply(mesh, dT, boxes, sig_fns, vv, vi, ii, iv, x0=x0, build=False)
+        m, mt = opgen.to_indexed(vv, vi, ii, iv, mt)
+        mat[x0 * n * n:x1 * n * n] = m
+    table = mt.table()
+    job = dict(name="large_plain_%d" % n, grid=[n, n, n], dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+               coefficients=dict(mat=mat, table=table))
+    if boxes:
+        job["pml"] = opgen.upml_apply(mesh, dT, boxes, sig_fns, build=True)
+    zr = (pml, n - 1 - pml) if pml else None   # Mur faces stop at the UPML slabs
+    job["mur"] = opgen.mur_dual(mesh, dT, [(0, "lo"), (0, "hi"), (1, "lo"), (1, "hi")], ranges=[None, None, zr])
+    sig = opgen.gauss_signal(f0, fc, dT, steps).astype(np.float32)
+    if tfsf:
+        def coef_at(kind, comp, flat):
+            return table[mat[flat], (3 if kind == "E" else 9) + comp].astype(np.float64)
+        lo = [tfsf_inset] * 3
+        hi = [n - 1 - tfsf_inset] * 3
+        vp, cp = opgen.tfsf_plane_wave(mesh, dT, lo, hi, (0, 0, 1), (1, 0, 0), coef_at, len(sig))
+        job["tfsf"] = dict(signal=sig, period=0, voltagePoints=vp, currentPoints=cp)
+    if nf2ff:
+        lo = [nf2ff_inset] * 3
+        hi = [n - 1 - nf2ff_inset] * 3
+        pts, meta, primal, dual = opgen.nf2ff_box(mesh, lo, hi)
+        freqs = [f0 + fc * (k - (nfreq - 1) / 2) / max(1, nfreq - 1) for k in range(nfreq)]
+        job["nf2ff"] = dict(surfaceIndices=pts.ravel(), numPoints=len(pts), omegas=[2 * math.pi * f for f in freqs],
+                            dT=dT, gridSize=[n, n, n], primalEdgeLens=primal, dualEdgeLens=dual, maxTS=steps,
+                            windowType=0)
+        job["nf2ff_meta"] = meta
+        job["nf2ff_freqs"] = freqs
+    return job
+
+
+def job_bytes_per_step(job):
+    """Algorithmic HBM bytes of one timestep of `job` (fields read+written once,
+    one u32 material index per cell, UPML/Mur/TFSF/NF2FF/probe traffic):
+    core 48 B + 4 B per cell; UPML 24 B flux r/w + 72 B coefficients per
+    region cell (3 components); Mur 3 passes ~ 28 B per point; TFSF/excitation
+    16 B per point; NF2FF 24 B field reads + 96 B accumulator r/w per
+    point-frequency."""
+    Nx, Ny, Nz = job["grid"]
+    N = Nx * Ny * Nz
+    coeff = 4 if "mat" in job["coefficients"] else 48
+    b = N * (48 + coeff)
+    for r in job.get("pml") or []:
+        c = r["numLines"][0] * r["numLines"][1] * r["numLines"][2]
+        b += c * (24 + 72)
+    if job.get("mur"):
+        b += 28 * (len(job["mur"]["coeff_nyP"]) + len(job["mur"]["coeff_nyPP"]))
+    if job.get("tfsf"):
+        t = job["tfsf"]
+        nv = len(t["voltagePoints"]["field_idx"]) if isinstance(t["voltagePoints"], dict) else len(t["voltagePoints"])
+        nc = len(t["currentPoints"]["field_idx"]) if isinstance(t["currentPoints"], dict) else len(t["currentPoints"])
+        b += 16 * (nv + nc)
+    if job.get("excitation"):
+        b += 16 * len(job["excitation"]["amp"])
+    if job.get("nf2ff"):
+        nf = job["nf2ff"]
+        b += nf["numPoints"] * (24 + 96 * len(nf.get("omegas") or [1]))
+    return b
+
+
+def configure(engine, job):
+    """The orchestrator's configure sequence (sim-engine.mjs:541-638)."""
+    engine.init(job["grid"], job["coefficients"])
+    if job.get("excitation"):
+        engine.configureExcitation(job["excitation"])
+    if job.get("pml"):
+        engine.configurePML(job["pml"])
+    if job.get("mur"):
+        engine.configureMur(job["mur"])
+    if job.get("tfsf"):
+        engine.configureTFSF(job["tfsf"])
+    if job.get("ade"):
+        engine.configureLorentzADE(job["ade"])
+    if job.get("pbc"):
+        engine.configurePBC(job["pbc"])
+    if job.get("nf2ff"):
+        engine.configureNF2FFAccumulation(job["nf2ff"])
+    probes = job.get("probes") or []
+    slices = None
+    if probes:
+        idx, slices = opgen.build_gather_indices(probes, job["grid"])
+        interval = probes[0]["processInterval"]
+        max_samples = int(math.ceil(job["maxTS"] / interval)) + 1
+        engine.configureProbeGatherBuffered(idx, maxSamples=max_samples, sampleInterval=interval)
+    return slices
+
+
+def run(engine, job, batch=100, on_energy=None):
+    """The orchestrator's stepping loop (sim-engine.mjs:640-681): iterate in
+    batches, check the lagged energy every 100 steps against endCrit."""
+    slices = configure(engine, job)
+    total, max_e = 0, 0.0
+    end = job.get("endCrit", 0.0) or 0.0
+    while total < job["maxTS"]:
+        n = min(batch, job["maxTS"] - total)
+        engine.iterate(n)
+        total += n
+        if total % 100 < n:
+            e = engine.computeEnergy()
+            if on_energy:
+                on_energy(total, e)
+            max_e = max(max_e, e)
+            if end > 0 and max_e > 0 and e / max_e <= end:
+                break
+    return total, slices
+
+
+def probe_series(engine, job, slices):
+    """Read the probe ring and integrate (sim-engine.mjs:683-696): (num_samples, num_probes)."""
+    r = engine.readProbeGatherBuffered()
+    if r is None:
+        return np.zeros((0, len(job["probes"])))
+    g = np.asarray(r["data"]).reshape(r["numSamples"], r["stride"])
+    return opgen.probe_integrals(g, job["probes"], slices)
+
+
+def run_probe_job(engine, job):
+    """Run a probe-only job; returns the first probe's series (with t = 0 if the
+    job's reference data starts there)."""
+    _, slices = run(engine, job, batch=job.get("batch", 100))
+    v = probe_series(engine, job, slices)[:, 0]
+    if job.get("include_t0"):
+        v = np.concatenate([[0.0], v])
+    return v

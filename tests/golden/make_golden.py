@@ -1,0 +1,30 @@
+"""Extract the golden vectors used by the parity tests from the reference's
+native-openEMS fixtures (reference tree: tests/fixtures/).
+
+Run in a checkout that has the reference at REF (default /root/reference);
+the outputs are committed so the tests never read the reference tree.
+  openems_cavity_vp.npy   engine_comparison/reference.json, engine "basic":
+                          probe voltage vp, 251 samples every 2 steps from t=0
+  openems_cavity_t.npy    the matching sample times (s)
+  constants.json          physical constants of the fixtures
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+fx = os.path.join(REF, "tests", "fixtures")
+ref = json.load(open(os.path.join(fx, "engine_comparison", "reference.json")))["engine_probes"]
+basic = ref["basic"]
+# the three native engines agree bit for bit (comparison.json); keep that check
+for other in ("sse", "sse-compressed"):
+    assert ref[other]["voltage"] == basic["voltage"]
+np.save(os.path.join(OUT, "openems_cavity_vp.npy"), np.asarray(basic["voltage"], np.float64))
+np.save(os.path.join(OUT, "openems_cavity_t.npy"), np.asarray(basic["time_s"], np.float64))
+with open(os.path.join(fx, "constants.json")) as f, open(os.path.join(OUT, "constants.json"), "w") as g:
+    g.write(f.read())
+print("wrote", OUT)

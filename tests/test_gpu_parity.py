@@ -1,0 +1,414 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+The CUDA kernels evaluate every update with separately rounded f32 multiplies
+and adds in the reference's operand order, so against the oracle's f32 mode
+the fields, UPML fluxes, Mur/ADE/RLC/steady-state state and the probe ring
+must agree BIT FOR BIT.  The NF2FF accumulators agree to 1e-6 relative (the
+per-step cosine/sine come from two f64 libraries), the energy to 1e-9 and the
+far field to 1e-4 (f32 sums in a different order against an f64 oracle).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, free_space, idx
+from oracle.oracle import OracleEngine, far_field
+
+pytestmark = pytest.mark.gpu
+
+
+def rand_coeffs(N, seed, pec_frac=0.05):
+    Nx, Ny, Nz = N
+    t = 3 * Nx * Ny * Nz
+    r = np.random.default_rng(seed)
+    c = dict(vv=(0.95 + 0.05 * r.random(t)).astype(np.float32), vi=(0.1 + 0.2 * r.random(t)).astype(np.float32),
+             ii=(0.97 + 0.03 * r.random(t)).astype(np.float32), iv=(0.1 + 0.2 * r.random(t)).astype(np.float32))
+    m = r.random(t) < pec_frac
+    c["vv"][m] = 0
+    c["vi"][m] = 0
+    return c
+
+
+def both(cuda_cls, N, coeffs, indexed=False):
+    g = cuda_cls()
+    assert g.initGPU()
+    if indexed:
+        from efs_b200 import opgen
+        vv, vi, ii, iv = [coeffs[k].reshape(3, *N) for k in ("vv", "vi", "ii", "iv")]
+        mat, mt = opgen.to_indexed(vv, vi, ii, iv)
+        g.init(N, dict(mat=mat, table=mt.table()))
+    else:
+        g.init(N, coeffs)
+    o = OracleEngine(N, coeffs, mode="f32")
+    return g, o
+
+
+def seed_fields(g, o, N, seed):
+    r = np.random.default_rng(seed)
+    n = 3 * N[0] * N[1] * N[2]
+    v = r.standard_normal(n).astype(np.float32)
+    c = r.standard_normal(n).astype(np.float32)
+    g.uploadFields(v, c)
+    o.uploadFields(v, c)
+
+
+def assert_bitexact(a, b, what):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    assert a.shape == b.shape, what
+    bad = np.flatnonzero(a.view(np.uint32) != b.view(np.uint32))
+    assert bad.size == 0, "%s: %d mismatches, first at %d: %r vs %r" % (what, bad.size, bad[0], a[bad[0]], b[bad[0]])
+
+
+def compare_fields(g, o, what=""):
+    f = g.getFields()
+    assert_bitexact(f["volt"], o.volt, what + " volt")
+    assert_bitexact(f["curr"], o.curr, what + " curr")
+
+
+@pytest.mark.parametrize("indexed", [False, True])
+@pytest.mark.parametrize("N", [(3, 3, 3), (8, 1, 1), (17, 9, 35), (33, 40, 70)])
+def test_core_bitexact(cuda_engine_cls, N, indexed):
+    c = rand_coeffs(N, 1) if not indexed else free_space(*N)
+    g, o = both(cuda_engine_cls, N, c, indexed)
+    seed_fields(g, o, N, 2)
+    for steps in (1, 5, 70):
+        g.iterate(steps)
+        o.iterate(steps)
+        compare_fields(g, o, "core %s +%d" % (N, steps))
+    assert g.numTS == o.numTS == 76
+
+
+def test_excitation_and_ring(cuda_engine_cls):
+    N = (12, 10, 14)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 3))
+    sig = np.sin(np.arange(37) * 0.4).astype(np.float32)
+    pos = [5 * 140 + 4 * 14 + 6, 2 * 140 + 3 * 14 + 7, 5 * 140 + 4 * 14 + 6]   # repeated target
+    exc = dict(signal=sig, delay=[0, 3, 1], amp=[1.0, -0.7, 0.25], dir=[2, 0, 2], pos=pos, period=0)
+    for e in (g, o):
+        e.configureExcitation(exc)
+    probe = [idx(2, 5, 4, 6, *N), idx(0, 1, 1, 1, *N), idx(1, 11, 9, 13, *N)]
+    g.configureProbeGatherBuffered(probe, maxSamples=20, sampleInterval=3)
+    o.configureProbeGatherBuffered(probe, 20, 3)
+    g.iterate(50)
+    o.iterate(50)
+    compare_fields(g, o, "excitation")
+    rg, ro = g.readProbeGatherBuffered(), o.readProbeGatherBuffered()
+    assert rg["numSamples"] == ro["numSamples"] == 16 and rg["stride"] == 6
+    assert_bitexact(rg["data"], ro["data"], "ring")
+    # periodic excitation, past-end semantics
+    g2, o2 = both(cuda_engine_cls, N, rand_coeffs(N, 4))
+    exc2 = dict(signal=sig[:9], delay=[2], amp=[0.5], dir=[1], pos=[3 * 140 + 3 * 14 + 3], period=5)
+    for e in (g2, o2):
+        e.configureExcitation(exc2)
+    g2.iterate(23)
+    o2.iterate(23)
+    compare_fields(g2, o2, "periodic excitation")
+
+
+def pml_region(start, num, seed):
+    r = np.random.default_rng(seed)
+    t = 3 * num[0] * num[1] * num[2]
+    return dict(startPos=list(start), numLines=list(num),
+                vv=(0.8 + 0.2 * r.random(t)).astype(np.float32), vvfo=(0.7 + 0.3 * r.random(t)).astype(np.float32),
+                vvfn=(1.0 + 0.3 * r.random(t)).astype(np.float32), ii=(0.8 + 0.2 * r.random(t)).astype(np.float32),
+                iifo=(0.7 + 0.3 * r.random(t)).astype(np.float32), iifn=(1.0 + 0.3 * r.random(t)).astype(np.float32))
+
+
+@pytest.mark.parametrize("overlap", [False, True])
+def test_pml_bitexact(cuda_engine_cls, overlap):
+    N = (20, 18, 24)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 5))
+    regs = [pml_region((0, 0, 0), (20, 18, 4), 6), pml_region((0, 0, 20), (20, 18, 4), 7),
+            pml_region((0, 0, 4), (4, 18, 16), 8)]
+    if overlap:
+        regs.append(pml_region((2, 3, 2), (6, 5, 7), 9))   # overlaps three others
+    for e in (g, o):
+        e.configurePML(regs)
+    seed_fields(g, o, N, 10)
+    g.iterate(25)
+    o.iterate(25)
+    compare_fields(g, o, "pml")
+    for r in range(len(regs)):
+        assert_bitexact(g.debugRead("pml_volt_flux", r), o.read("pml_volt_flux", r), "vflux %d" % r)
+        assert_bitexact(g.debugRead("pml_curr_flux", r), o.read("pml_curr_flux", r), "cflux %d" % r)
+
+
+def mur_faces(N, coeff_seed):
+    """Dual-component Mur on the x and y faces, with coinciding normals at the corners."""
+    Nx, Ny, Nz = N
+    r = np.random.default_rng(coeff_seed)
+    nP, sP, nPP, sPP = [], [], [], []
+    for ny, line, shift in ((0, 0, 1), (0, Nx - 1, Nx - 2), (1, 0, 1), (1, Ny - 1, Ny - 2)):
+        P, PP = (ny + 1) % 3, (ny + 2) % 3
+        nl = [Nx, Ny, Nz]
+        for i1 in range(nl[PP]):
+            for i0 in range(nl[P]):
+                pos = [0, 0, 0]
+                pos[ny], pos[P], pos[PP] = line, i0, i1
+                sh = list(pos)
+                sh[ny] = shift
+                nP.append(idx(P, *pos, *N)); sP.append(idx(P, *sh, *N))
+                nPP.append(idx(PP, *pos, *N)); sPP.append(idx(PP, *sh, *N))
+    return dict(coeff_nyP=(r.random(len(nP)) * 0.5).astype(np.float32), coeff_nyPP=(r.random(len(nPP)) * 0.5).astype(np.float32),
+                normal_idx_nyP=nP, shifted_idx_nyP=sP, normal_idx_nyPP=nPP, shifted_idx_nyPP=sPP)
+
+
+def test_mur_with_pml_corners_bitexact(cuda_engine_cls):
+    N = (14, 12, 20)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 11))
+    regs = [pml_region((0, 0, 0), (14, 12, 3), 12), pml_region((0, 0, 17), (14, 12, 3), 13)]
+    mur = mur_faces(N, 14)
+    for e in (g, o):
+        e.configurePML(regs)
+        e.configureMur(mur)
+    seed_fields(g, o, N, 15)
+    g.iterate(30)
+    o.iterate(30)
+    compare_fields(g, o, "mur")
+    assert_bitexact(g.debugRead("mur_saved"), o.read("mur_saved"), "mur_saved")
+
+
+def test_tfsf_bitexact(cuda_engine_cls):
+    N = (10, 11, 12)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 16))
+    r = np.random.default_rng(17)
+    vp = [dict(field_idx=int(r.integers(0, 3 * 1320)), delay_int=int(r.integers(0, 6)), delay_frac=float(r.random()),
+               amp=float(r.standard_normal())) for _ in range(60)]
+    vp.append(dict(vp[0]))          # duplicate target, applied in order
+    cp = [dict(field_idx=int(r.integers(0, 3 * 1320)), delay_int=int(r.integers(0, 6)), delay_frac=float(r.random()),
+               amp=float(r.standard_normal())) for _ in range(40)]
+    cfg = dict(signal=np.cos(np.arange(25) * 0.5).astype(np.float32), period=0, voltagePoints=vp, currentPoints=cp)
+    for e in (g, o):
+        e.configureTFSF(cfg)
+    g.iterate(35)
+    o.iterate(35)
+    compare_fields(g, o, "tfsf")
+
+
+def test_ade_in_and_out_of_pml_bitexact(cuda_engine_cls):
+    N = (12, 10, 16)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 18))
+    regs = [pml_region((0, 0, 0), (12, 10, 4), 19)]
+    r = np.random.default_rng(20)
+    cells = r.choice(12 * 10 * 16, 80, replace=False)   # some inside the UPML slab
+    orders = []
+    for lor in (False, True):
+        dirs = []
+        for d in range(3):
+            k = len(cells)
+            dirs.append(dict(dir=d, pos_idx=cells, v_int_ADE=r.random(k) * 0.9, v_ext_ADE=r.random(k) * 0.3,
+                             v_Lor_ADE=r.random(k) * 0.1, i_int_ADE=r.random(k) * 0.9, i_ext_ADE=r.random(k) * 0.3,
+                             i_Lor_ADE=r.random(k) * 0.1))
+        orders.append(dict(numCells=len(cells), hasLorentz=lor, directions=dirs))
+    for e in (g, o):
+        e.configurePML(regs)
+        e.configureLorentzADE({"orders": orders})
+    seed_fields(g, o, N, 21)
+    g.iterate(12)
+    o.iterate(12)
+    compare_fields(g, o, "ade")
+    for name in ("ade_volt", "ade_volt_lor", "ade_curr", "ade_curr_lor"):
+        ref = np.concatenate([o.read(name, oi, d) for oi in range(2) for d in range(3)])
+        assert_bitexact(g.debugRead(name), ref, name)
+
+
+def test_rlc_bitexact(cuda_engine_cls):
+    N = (8, 8, 8)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 22))
+    r = np.random.default_rng(23)
+    els = []
+    for k in range(12):
+        els.append(dict(field_idx=int(r.integers(0, 512)), direction=int(r.integers(0, 3)), type_flag=int(k % 2),
+                        i2v=float(r.random()), ilv=float(r.random() * 0.1), vvd=float(0.5 + 0.4 * r.random()),
+                        vv2=float(r.random() * 0.1), vj1=float(r.random() * 0.1), vj2=float(r.random() * 0.1),
+                        ib0=float(r.random() * 0.3), b1=float(r.random() * 0.1), b2=float(r.random() * 0.1)))
+    els.append(dict(els[1]))        # two series elements on one edge: sequential
+    for e in (g, o):
+        e.configureRLC(dict(elements=els))
+    seed_fields(g, o, N, 24)
+    g.iterate(20)
+    o.iterate(20)
+    compare_fields(g, o, "rlc")
+    for name in ("rlc_vdn", "rlc_jn", "rlc_vil"):
+        assert_bitexact(g.debugRead(name), o.read(name), name)
+
+
+def test_steady_state_bitexact(cuda_engine_cls):
+    N = (9, 9, 9)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 25))
+    probes = [idx(0, 4, 4, 4, *N), idx(2, 3, 5, 2, *N)]
+    cfg = dict(probe_idx=probes, periodSamples=4, threshold=1e-3)
+    for e in (g, o):
+        e.configureSteadyState(cfg)
+    seed_fields(g, o, N, 26)
+    g.iterate(3)
+    o.iterate(3)
+    g.setSteadyStateRecording(True)
+    o.setSteadyState(True)
+    g.iterate(6)
+    o.iterate(6)
+    g.setSteadyStateRecording(False)
+    o.setSteadyState(False)
+    g.iterate(2)
+    o.iterate(2)
+    s = g.readSteadyState()
+    assert s["currentSample"] == o.steadyStateSample == 6
+    assert_bitexact(s["energy_period1"], o.read("ss_e1"), "ss_e1")
+    assert_bitexact(s["energy_period2"], o.read("ss_e2"), "ss_e2")
+    assert s["converged"] == o.checkConvergence()
+
+
+@pytest.mark.parametrize("phase", [0.0, 0.7])
+def test_pbc_bitexact(cuda_engine_cls, phase):
+    N = (10, 12, 9)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 27, pec_frac=0))
+    cfg = dict(axes=[dict(axis=0, phase=phase), dict(axis=2, phase=0.0)])
+    for e in (g, o):
+        e.configurePBC(cfg)
+    seed_fields(g, o, N, 28)
+    g.iterate(15)
+    o.iterate(15)
+    compare_fields(g, o, "pbc")
+    if phase:
+        assert_bitexact(g.debugRead("pbc_imag"), o.read("pbc_imag"), "pbc_imag")
+
+
+def nf2ff_inputs(N, lines_delta=1e-3, nfreq=3, inset=2):
+    """Points on the six faces of a box `inset` cells inside the grid."""
+    Nx, Ny, Nz = N
+    lo = [inset] * 3
+    hi = [Nx - 1 - inset, Ny - 1 - inset, Nz - 1 - inset]
+    pts = []
+    for d in range(3):
+        for face in (lo[d], hi[d]):
+            rng = [range(lo[k], hi[k] + 1) if k != d else [face] for k in range(3)]
+            for x in rng[0]:
+                for y in rng[1]:
+                    for z in rng[2]:
+                        pts.append((x, y, z))
+    pts = np.asarray(pts, np.uint32)
+    el = []
+    for n in range(3):
+        e = np.full(N[n], lines_delta, np.float32)
+        el.append(e)
+    dual = []
+    for n in range(3):
+        d = np.full(N[n], lines_delta, np.float32)
+        d[0] = d[-1] = 0.5 * lines_delta
+        dual.append(d)
+    return dict(surfaceIndices=pts.ravel(), numPoints=len(pts), omegas=[2e10 * (k + 1) for k in range(nfreq)],
+                dT=1.5e-12, gridSize=list(N), primalEdgeLens=el, dualEdgeLens=dual, maxTS=400, windowType=0)
+
+
+@pytest.mark.parametrize("window", [0, 1])
+def test_nf2ff_accumulation(cuda_engine_cls, window):
+    N = (14, 13, 15)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 29, pec_frac=0))
+    cfg = nf2ff_inputs(N)
+    cfg["windowType"] = window
+    g.configureNF2FFAccumulation(cfg)
+    o.configureNF2FFAccumulation(cfg)
+    seed_fields(g, o, N, 30)
+    g.iterate(40)
+    o.iterate(40)
+    compare_fields(g, o, "nf2ff fields")
+    ag, ao = g.readNF2FFAccumulation(True), o.readNF2FFAccumulation(True)
+    for k in ("accumE", "accumH"):
+        a, b = np.asarray(ag[k], np.float64), np.asarray(ao[k], np.float64)
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), k
+
+
+def test_far_field_against_f64(cuda_engine_cls):
+    N = (14, 13, 15)
+    g, _ = both(cuda_engine_cls, N, rand_coeffs(N, 31, pec_frac=0))
+    cfg = nf2ff_inputs(N, nfreq=2)
+    g.configureNF2FFAccumulation(cfg)
+    seed_fields(g, _, N, 32)
+    g.iterate(30)
+    acc = g.readNF2FFAccumulation(True)
+    pts = cfg["surfaceIndices"].reshape(-1, 3).astype(np.float64) * 1e-3
+    r = np.random.default_rng(33)
+    meta = np.zeros((cfg["numPoints"], 8), np.float32)
+    meta[:, :3] = pts
+    meta[:, 3] = r.integers(0, 3, cfg["numPoints"])
+    meta[:, 4] = r.choice([-1.0, 1.0], cfg["numPoints"])
+    meta[:, 5] = 1e-6
+    theta = np.deg2rad(np.arange(0, 181, 15)).astype(np.float32)
+    phi = np.deg2rad(np.arange(0, 361, 20)).astype(np.float32)
+    for fi in range(2):
+        out = g.computeNF2FFfarField(dict(pointMeta=meta, theta=theta, phi=phi, center=[7e-3, 6e-3, 7e-3],
+                                          frequency=cfg["omegas"][fi] / (2 * np.pi), radius=1.0,
+                                          numPoints=cfg["numPoints"], freqIndex=fi)).reshape(-1, 5)
+        ref = far_field(acc["accumE"][fi], acc["accumH"][fi], meta, theta, phi, cfg["omegas"][fi] / (2 * np.pi),
+                        1.0, (7e-3, 6e-3, 7e-3))
+        scale = np.abs(ref[:, 1:]).max()
+        assert np.abs(out[:, 1:] - ref[:, 1:]).max() <= 1e-4 * scale
+        assert np.abs(out[:, 0] - ref[:, 0]).max() <= 2e-4 * ref[:, 0].max()
+
+
+def test_energy_and_lag(cuda_engine_cls):
+    N = (11, 12, 13)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 34))
+    seed_fields(g, o, N, 35)
+    assert g.computeEnergy() == 0.0          # first lagged call returns 0 (:2995-3020)
+    e0 = o.energy()
+    g.iterate(4)
+    o.iterate(4)
+    assert abs(g.computeEnergy() - e0) <= 1e-9 * e0
+    e1 = o.energy()
+    assert abs(g.flushEnergy() - e1) <= 1e-9 * e1
+    assert abs(g.computeEnergy(lagged=False) - e1) <= 1e-9 * e1
+
+
+def test_state_roundtrip(cuda_engine_cls):
+    N = (10, 9, 12)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 36))
+    regs = [pml_region((0, 0, 0), (10, 9, 3), 37)]
+    g.configurePML(regs)
+    g.configureNF2FFAccumulation(nf2ff_inputs(N, nfreq=1))
+    seed_fields(g, o, N, 38)
+    g.iterate(7)
+    blob = g.getState()
+    f7 = g.getFields()
+    g.iterate(5)
+    f12 = g.getFields()
+    g.setState(blob)
+    assert g.numTS == 7
+    assert_bitexact(g.getFields()["volt"], f7["volt"], "restored")
+    g.iterate(5)
+    assert_bitexact(g.getFields()["curr"], f12["curr"], "replayed")
+
+
+def test_invalid_inputs_raise(cuda_engine_cls):
+    from efs_b200.engine import EfsError
+    g = cuda_engine_cls()
+    assert g.initGPU()
+    with pytest.raises(EfsError):
+        g.iterate(1)                      # before init: EFS_ERR_STATE
+    N = (4, 4, 4)
+    g.init(N, free_space(*N))
+    with pytest.raises(EfsError):
+        g.configureExcitation(dict(signal=[1.0], delay=[0], amp=[1.0], dir=[3], pos=[0], period=0))
+    with pytest.raises(EfsError):
+        g.configureMur(dict(coeff=0.1, normal_idx=[3 * 64], shifted_idx=[0]))
+    with pytest.raises(EfsError):
+        g.configurePML([pml_region((2, 0, 0), (3, 4, 4), 1)])
+    g.iterate(2)                          # engine still usable
+    assert g.numTS == 2
+
+
+def test_openems_cavity_fixture_on_gpu(cuda_engine_cls):
+    """Native-openEMS engine_comparison cavity (tests/fixtures/engine_comparison,
+    16x8x18 PEC box, 500 steps) reproduced by the CUDA engine: relative L2 of
+    the probe voltage < 1e-4."""
+    from efs_b200 import workloads
+    job = workloads.openems_cavity()
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "openems_cavity_vp.npy"))
+    g = cuda_engine_cls()
+    assert g.initGPU()
+    v = workloads.run_probe_job(g, job)
+    err = np.linalg.norm(v - ref) / np.linalg.norm(ref)
+    assert err < 1e-4, err
