@@ -567,14 +567,17 @@ def tfsf_plane_wave(mesh, dT, lo, hi, k_hat, e_hat, coef_at, signal_len, E0=1.0)
             r.append(c[np.clip(p[a], 0, len(c) - 1)])
         return np.stack(r, axis=-1)
 
-    # candidate nodes: a shell of thickness 2 around the box surface
-    axes_r = [np.arange(max(lo[a] - 2, 0), min(hi[a] + 3, mesh.shape[a])) for a in range(3)]
-    P = np.meshgrid(*axes_r, indexing="ij")
-    P = [p.ravel() for p in P]
-    near = np.zeros(P[0].shape, bool)
+    # candidate nodes: the union of six slabs (thickness 3) around the box faces
+    span = [np.arange(max(lo[a] - 2, 0), min(hi[a] + 3, mesh.shape[a])) for a in range(3)]
+    flats = []
     for a in range(3):
-        near |= (np.abs(P[a] - lo[a]) <= 1) | (np.abs(P[a] - hi[a]) <= 1)
-    P = [p[near] for p in P]
+        for c in (lo[a], hi[a]):
+            rr = list(span)
+            rr[a] = np.arange(max(c - 1, 0), min(c + 2, mesh.shape[a]))
+            g = np.meshgrid(*rr, indexing="ij")
+            flats.append((g[0] * Ny + g[1]).astype(np.int64).ravel() * Nz + g[2].ravel())
+    flat_all = np.unique(np.concatenate(flats))
+    P = [flat_all // (Ny * Nz), (flat_all // Nz) % Ny, flat_all % Nz]
     vpts, cpts = [], []
     for n in range(3):
         # E edges inside whose curl reads an H edge outside

@@ -10,6 +10,7 @@ WebGPUEngine method names (the CUDA engine, or the CPU oracle in tests), and
 check, probe readback, :648-696).
 """
 import math
+import os
 
 import numpy as np
 
@@ -46,15 +47,51 @@ def openems_cavity():
                 probes=[probe], include_t0=True)
 
 
-class _LazyCells:
-    """Per-cell property looked up from a uint8 material-id grid on slicing."""
+class _ChunkCells:
+    """Per-cell eps_r of the cells with x index in [xs, xe), looked up by global x slice."""
 
-    def __init__(self, ids, values):
-        self.ids = ids
+    def __init__(self, ids, xs, values):
+        self.ids, self.xs = ids, xs
         self.values = np.asarray(values, np.float64)
 
     def __getitem__(self, sl):
-        return self.values[self.ids[sl]]
+        return self.values[self.ids[sl.start - self.xs:sl.stop - self.xs]]
+
+
+def _large_plain_chunk(args):
+    """Operator rows of x-planes [x0, x1) for large_plain (runs in a worker)."""
+    n, delta, dT, x0, x1, diel, eps_vals, pec_boxes, pml = args
+    lines = opgen.uniform_lines(n, delta)
+    mesh = opgen.Mesh(lines, lines, lines)
+    xs, xe = max(x0 - 1, 0), min(x1, n - 1)
+    ids = np.zeros((xe - xs, n - 1, n - 1), np.uint8)
+    for k, (lo, hi) in enumerate(diel):
+        a, b = max(lo[0], xs), min(hi[0], xe)
+        if a < b:
+            ids[a - xs:b - xs, lo[1]:hi[1], lo[2]:hi[2]] = k + 1
+
+    def pec(nn, c0, c1):
+        m = np.zeros((c1 - c0, n, n), bool)
+        for lo, hi in pec_boxes:
+            m |= opgen.edge_mask_in_box(mesh, nn, lo, hi, xslice=slice(c0, c1))
+        return m
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, eps_r=_ChunkCells(ids, xs, eps_vals), pec_edges=pec,
+                                          bc=(2, 2, 2, 2, 3, 3), x0=x0, x1=x1)
+    if pml:
+        boxes = [((0, 0, 0), (n, n, pml)), ((0, 0, n - pml), (n, n, pml))]
+        opgen.upml_apply(mesh, dT, boxes, [None, None, opgen.pml_sigma(mesh, 2, pml, pml)], vv, vi, ii, iv,
+                         x0=x0, build=False)
+    m, mt = opgen.to_indexed(vv, vi, ii, iv)
+    return x0, x1, m, mt.table()
+
+
+def _parallel_map(fn, items, workers):
+    if workers <= 1 or len(items) <= 1:
+        return [fn(a) for a in items]
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")          # never fork a process that may hold a CUDA context
+    with ctx.Pool(workers) as pool:
+        return pool.map(fn, items, chunksize=1)
 
 
 def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_inset=20, nf2ff_inset=10,
@@ -72,9 +109,8 @@ def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_ins
     dT = opgen.cfl_dt(mesh)
     rng = np.random.default_rng(seed)
     nc = n - 1
-    ids = np.zeros((nc, nc, nc), np.uint8)
     eps_vals = [1.0]
-    pec_boxes = []
+    pec_boxes, diel = [], []
     margin = tfsf_inset + 4
     lo_cap = max(margin, 1)
     for i in range(nboxes):
@@ -85,26 +121,16 @@ def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_ins
             pec_boxes.append(([lines[lo[a]] for a in range(3)], [lines[hi[a]] for a in range(3)]))
         else:
             eps_vals.append(float(rng.uniform(2.0, 10.0)))
-            ids[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = len(eps_vals) - 1
-    eps = _LazyCells(ids, eps_vals)
-
-    def pec(nn, x0, x1):
-        m = np.zeros((x1 - x0, n, n), bool)
-        for lo, hi in pec_boxes:
-            m |= opgen.edge_mask_in_box(mesh, nn, lo, hi, xslice=slice(x0, x1))
-        return m
-    bc = (2, 2, 2, 2, 3, 3)
+            diel.append((lo.tolist(), hi.tolist()))
     boxes = [((0, 0, 0), (n, n, pml)), ((0, 0, n - pml), (n, n, pml))] if pml else []
     sig_fns = [None, None, opgen.pml_sigma(mesh, 2, pml, pml)] if pml else [None] * 3
+    items = [(n, delta, dT, x0, min(n, x0 + chunk), diel, eps_vals, pec_boxes, pml) for x0 in range(0, n, chunk)]
+    workers = min(len(items), max(1, (os.cpu_count() or 1)), 32) if n >= 128 else 1
     mt = opgen.MaterialTable()
     mat = np.empty(n * n * n, np.uint32)
-    for x0 in range(0, n, chunk):
-        x1 = min(n, x0 + chunk)
-        vv, vi, ii, iv = opgen.operator_dense(mesh, dT, eps_r=eps, pec_edges=pec, bc=bc, x0=x0, x1=x1)
-        if boxes:
-            opgen.upml_apply(mesh, dT, boxes, sig_fns, vv, vi, ii, iv, x0=x0, build=False)
-        m, mt = opgen.to_indexed(vv, vi, ii, iv, mt)
-        mat[x0 * n * n:x1 * n * n] = m
+    for x0, x1, m, tab in _parallel_map(_large_plain_chunk, items, workers):
+        remap = mt.add(tab)
+        mat[x0 * n * n:x1 * n * n] = remap[m]
     table = mt.table()
     job = dict(name="large_plain_%d" % n, grid=[n, n, n], dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
                coefficients=dict(mat=mat, table=table))

@@ -4,7 +4,7 @@ The CUDA kernels evaluate every update with separately rounded f32 multiplies
 and adds in the reference's operand order, so against the oracle's f32 mode
 the fields, UPML fluxes, Mur/ADE/RLC/steady-state state and the probe ring
 must agree BIT FOR BIT.  The NF2FF accumulators agree to 1e-6 relative (the
-per-step cosine/sine come from two f64 libraries), the energy to 1e-9 and the
+per-step cosine/sine come from two f64 libraries), the energy to 1e-7 and the
 far field to 1e-4 (f32 sums in a different order against an f64 oracle).
 """
 import json
@@ -357,10 +357,10 @@ def test_energy_and_lag(cuda_engine_cls):
     e0 = o.energy()
     g.iterate(4)
     o.iterate(4)
-    assert abs(g.computeEnergy() - e0) <= 1e-9 * e0
+    assert abs(g.computeEnergy() - e0) <= 1e-7 * e0   # f32 per-cell partials vs f64 (reference bar: 1e-4)
     e1 = o.energy()
-    assert abs(g.flushEnergy() - e1) <= 1e-9 * e1
-    assert abs(g.computeEnergy(lagged=False) - e1) <= 1e-9 * e1
+    assert abs(g.flushEnergy() - e1) <= 1e-7 * e1
+    assert abs(g.computeEnergy(lagged=False) - e1) <= 1e-7 * e1
 
 
 def test_state_roundtrip(cuda_engine_cls):
