@@ -20,6 +20,7 @@
 // CUDA graph of the whole step sequence.
 #include "../../include/efs.h"
 #include "efs_kernels.cuh"
+#include "efs_fused.cuh"
 
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -83,7 +84,15 @@ struct efs_engine {
     bool inited = false;
     uint32_t Nx = 0, Ny = 0, Nz = 0;
     size_t N = 0;
-    DevBuf volt, curr;
+    DevBuf volt, curr;          // fields (parity 0)
+    DevBuf volt_b, curr_b;      // second buffers of the fused path (parity 1)
+    bool fused = true;          // single-pass E+H kernel (else separate E and H sweeps)
+    int cur = 0;                // parity holding the current fields
+    uint32_t xchunk = 64;       // x-planes per block of the fused kernel
+    int cpt = 2;                // z cells per thread of the fused kernel
+    DevBuf defer_bits, defer_cells;
+    uint32_t defer_n = 0;
+    std::vector<uint32_t> h_exc_targets, h_tfsf_v_targets, h_mur_apply, h_rlc_series;
     bool indexed = false;
     DevBuf mat, table, vv, vi, ii, iv;
     uint32_t ntable = 0;
@@ -100,10 +109,18 @@ struct efs_engine {
     struct Region {
         uint32_t s[3], n[3];
         size_t total;
-        DevBuf vv, vvfo, vvfn, ii, iifo, iifn, vflux, cflux;
+        DevBuf vv, vvfo, vvfn, ii, iifo, iifn, vflux, cflux, vflux_b, cflux_b;
+        float* vf(int p) const { return (p && vflux_b.p) ? vflux_b.as<float>() : vflux.as<float>(); }
+        float* cf(int p) const { return (p && cflux_b.p) ? cflux_b.as<float>() : cflux.as<float>(); }
     };
     std::vector<std::unique_ptr<Region>> pml;
-    DevBuf vflux_ptrs, cflux_ptrs;
+    DevBuf vflux_ptrs[2], cflux_ptrs[2];
+
+    float* vbuf(int p) const { return (p && volt_b.p) ? volt_b.as<float>() : volt.as<float>(); }
+    float* cbuf(int p) const { return (p && curr_b.p) ? curr_b.as<float>() : curr.as<float>(); }
+    float* vcur() const { return vbuf(cur); }
+    float* ccur() const { return cbuf(cur); }
+    int pnext(int p) const { return fused ? 1 - p : p; }
 
     // Mur (host copies kept to rebuild read redirects)
     bool mur_on = false;
@@ -205,16 +222,27 @@ struct efs_engine {
             if (p[i] >= 3 * N) fail(EFS_ERR_INVALID, std::string(what) + ": index out of range");
     }
 
-    Grid grid() const {
+    Grid grid(int p = 0) const {
         Grid g;
         g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.indexed = indexed;
         g.N = N; g.NyNz = (size_t)Ny * Nz;
-        g.volt = volt.as<float>(); g.curr = curr.as<float>();
+        g.volt = vbuf(p); g.curr = cbuf(p);
         g.mat = mat.as<uint32_t>(); g.table = table.as<float>();
         g.vv = vv.as<float>(); g.vi = vi.as<float>(); g.ii = ii.as<float>(); g.iv = iv.as<float>();
         return g;
     }
-    PmlSet pml_set() const {
+    FusedGrid fused_grid(int p) const {
+        FusedGrid g;
+        g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.xchunk = xchunk;
+        g.N = N; g.NyNz = (size_t)Ny * Nz;
+        g.V0 = vbuf(p); g.H0 = cbuf(p); g.V1 = vbuf(1 - p); g.H1 = cbuf(1 - p);
+        g.mat = mat.as<uint32_t>(); g.table = table.as<float>();
+        g.vv = vv.as<float>(); g.vi = vi.as<float>(); g.ii = ii.as<float>(); g.iv = iv.as<float>();
+        g.defer = defer_n ? defer_bits.as<uint32_t>() : nullptr;
+        return g;
+    }
+    // UPML set whose flux pointers are the parity-p buffers
+    PmlSet pml_set(int p = 0) const {
         PmlSet s;
         memset(&s, 0, sizeof(s));
         s.count = (int)pml.size();
@@ -223,7 +251,7 @@ struct efs_engine {
             for (int d = 0; d < 3; ++d) { s.r[r].s[d] = R.s[d]; s.r[r].n[d] = R.n[d]; }
             s.r[r].vv = R.vv.as<float>(); s.r[r].vvfo = R.vvfo.as<float>(); s.r[r].vvfn = R.vvfn.as<float>();
             s.r[r].ii = R.ii.as<float>(); s.r[r].iifo = R.iifo.as<float>(); s.r[r].iifn = R.iifn.as<float>();
-            s.r[r].vflux = R.vflux.as<float>(); s.r[r].cflux = R.cflux.as<float>();
+            s.r[r].vflux = R.vf(p); s.r[r].cflux = R.cf(p);
         }
         return s;
     }
@@ -252,11 +280,14 @@ struct efs_engine {
     // Rebuild everything that depends on more than one configure call.
     void build_plan() {
         if (!plan_dirty) return;
-        std::vector<float*> vp, cp;
-        for (auto& r : pml) { vp.push_back(r->vflux.as<float>()); cp.push_back(r->cflux.as<float>()); }
-        if (vp.empty()) { vp.push_back(nullptr); cp.push_back(nullptr); }
-        upload(vflux_ptrs, vp);
-        upload(cflux_ptrs, cp);
+        for (int p = 0; p < 2; ++p) {
+            std::vector<float*> vp, cp;
+            for (auto& r : pml) { vp.push_back(r->vf(p)); cp.push_back(r->cf(p)); }
+            if (vp.empty()) { vp.push_back(nullptr); cp.push_back(nullptr); }
+            upload(vflux_ptrs[p], vp);
+            upload(cflux_ptrs[p], cp);
+        }
+        build_deferred();
         if (mur_on) {
             std::vector<ReadLoc> rn(mur_n), rs(mur_n);
             for (uint32_t i = 0; i < mur_n; ++i) { rn[i] = redirect(h_mur_normal[i]); rs[i] = redirect(h_mur_shifted[i]); }
@@ -272,16 +303,73 @@ struct efs_engine {
         plan_dirty = false;
     }
 
-    // Enqueue timestep k of a batch (numTS = state.numTS + k).
-    void enqueue_step(uint32_t k) {
-        const Grid g = grid();
-        const PmlSet ps = pml_set();
+    // Fused path: H cells whose curl reads an E value rewritten by a sparse
+    // post-update operation (TFSF, PBC, Mur apply, excitation, series RLC)
+    // are updated after those operations by k_deferred_h.
+    void build_deferred() {
+        defer_n = 0;
+        if (!fused) return;
+        std::vector<uint32_t> mod;   // modified E entries as n*N + cell
+        auto add = [&](const std::vector<uint32_t>& v) { mod.insert(mod.end(), v.begin(), v.end()); };
+        if (tfsf_on) add(h_tfsf_v_targets);
+        if (exc_on) add(h_exc_targets);
+        if (mur_on) add(h_mur_apply);
+        if (rlc_on) add(h_rlc_series);
+        const uint32_t nl[3] = {Nx, Ny, Nz};
+        const size_t NyNz = (size_t)Ny * Nz;
+        if (pbc_on)
+            for (auto& a : pbc_axes) {
+                uint32_t t0 = (a.axis + 1) % 3, t1 = (a.axis + 2) % 3;
+                for (uint32_t i0 = 0; i0 < nl[t0]; ++i0)
+                    for (uint32_t i1 = 0; i1 < nl[t1]; ++i1) {
+                        uint32_t p[3];
+                        p[a.axis] = 0; p[t0] = i0; p[t1] = i1;
+                        if (a.axis == 1) { p[0] = i1; p[2] = i0; }   // face_to_grid order of the reference
+                        size_t c = p[0] * NyNz + (size_t)p[1] * Nz + p[2];
+                        mod.push_back((uint32_t)(t0 * N + c));
+                        mod.push_back((uint32_t)(t1 * N + c));
+                    }
+            }
+        if (mod.empty()) return;
+        std::vector<uint32_t> bits((N + 31) / 32, 0);
+        auto mark = [&](int64_t x, int64_t y, int64_t z) {
+            if (x < 0 || y < 0 || z < 0) return;
+            size_t c = (size_t)x * NyNz + (size_t)y * Nz + (size_t)z;
+            bits[c >> 5] |= 1u << (c & 31);
+        };
+        for (uint32_t f : mod) {
+            uint32_t n = f / (uint32_t)N;
+            size_t cell = f - (size_t)n * N;
+            int64_t x = cell / NyNz, y = (cell / Nz) % Ny, z = cell % Nz;
+            // E_n(m) appears in the curls of H at m, m - e_a, m - e_b (a, b != n)
+            mark(x, y, z);
+            if (n != 0) mark(x - 1, y, z);
+            if (n != 1) mark(x, y - 1, z);
+            if (n != 2) mark(x, y, z - 1);
+        }
+        std::vector<uint32_t> cells;
+        for (size_t w = 0; w < bits.size(); ++w)
+            for (uint32_t b = bits[w]; b; b &= b - 1) cells.push_back((uint32_t)(w * 32 + __builtin_ctz(b)));
+        upload(defer_bits, bits);
+        upload(defer_cells, cells);
+        defer_n = (uint32_t)cells.size();
+    }
+
+    // Enqueue timestep k of a batch (numTS = state.numTS + k); the fields are
+    // read from parity p and, on the fused path, written to parity 1 - p.
+    void enqueue_step(uint32_t k, int p) {
+        const int q = pnext(p);
+        const Grid g = grid(p);
+        const PmlSet ps = pml_set(p);
+        const PmlSet pn = pml_set(q);
         StepState* st = state.as<StepState>();
-        float* V = volt.as<float>();
-        float* C = curr.as<float>();
+        float* V = vbuf(p);          // E before the core update
+        float* C = cbuf(p);          // H before the core update
+        float* V1 = vbuf(q);         // E after it
+        float* C1 = cbuf(q);         // H after it
         const uint32_t T = 256;
-        const float* const* vfl = vflux_ptrs.as<const float*>();
-        const float* const* cfl = cflux_ptrs.as<const float*>();
+        const float* const* vfl = vflux_ptrs[p].as<const float*>();
+        const float* const* cfl = cflux_ptrs[p].as<const float*>();
 
         // --- pre-voltage ---
         if (ss_on)
@@ -292,35 +380,68 @@ struct efs_engine {
         if (mur_on) k_mur_pre<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
         RlcDev rd = rlc_dev();
         if (rlc_on) k_rlc_pre<<<blocks(rlc_n, T), T, 0, stream>>>(rd);
-        // --- core E (+UPML) ---
-        dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
         const bool hp = !pml.empty();
-        if (indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, stream>>>(g, ps); }
-        else { if (hp) k_volt<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, stream>>>(g, ps); }
-        // --- post-voltage / apply ---
-        if (tfsf_on && tfsf_v.groups) k_point_sources<1><<<blocks(tfsf_v.groups, T), T, 0, stream>>>(V, st, k, point_dev(tfsf_v, tfsf_signal, tfsf_len, tfsf_period));
-        if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, true);
-        if (mur_on) k_mur_post<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
+        if (fused) {
+            // ADE(curr) reads H and the current flux, which the E side never
+            // touches: it runs before the fused kernel overwrites the flux.
+            if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            launch_fused(p);
+        } else {
+            dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
+            if (indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, stream>>>(g, ps); }
+            else { if (hp) k_volt<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, stream>>>(g, ps); }
+        }
+        // --- post-voltage / apply (on the updated E) ---
+        if (tfsf_on && tfsf_v.groups) k_point_sources<1><<<blocks(tfsf_v.groups, T), T, 0, stream>>>(V1, st, k, point_dev(tfsf_v, tfsf_signal, tfsf_len, tfsf_period));
+        if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, true, V1);
+        if (mur_on) k_mur_post<<<blocks(mur_n, T), T, 0, stream>>>(V1, md);
         if (exc_on && exc_groups) {
             PointSources s{exc_groups, exc_target.as<uint32_t>(), exc_off.as<uint32_t>(), exc_delay.as<uint32_t>(),
                            exc_amp.as<float>(), nullptr, exc_signal.as<float>(), exc_len, exc_period};
-            k_point_sources<0><<<blocks(exc_groups, T), T, 0, stream>>>(V, st, k, s);
+            k_point_sources<0><<<blocks(exc_groups, T), T, 0, stream>>>(V1, st, k, s);
         }
-        if (mur_on) k_mur_apply<<<blocks(mur_napply, T), T, 0, stream>>>(V, md);
-        if (rlc_on) k_rlc_apply<<<blocks(rlc_groups, T), T, 0, stream>>>(V, rd);
-        // --- pre-current ---
-        if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
-        // --- core H (+UPML) ---
-        if (indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, stream>>>(g, ps); }
-        else { if (hp) k_curr<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<false, false><<<cg, cb, 0, stream>>>(g, ps); }
-        // --- post-current ---
-        if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
-        if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, false);
+        if (mur_on) k_mur_apply<<<blocks(mur_napply, T), T, 0, stream>>>(V1, md);
+        if (rlc_on) k_rlc_apply<<<blocks(rlc_groups, T), T, 0, stream>>>(V1, rd);
+        if (fused) {
+            if (defer_n) {
+                const FusedGrid fg = fused_grid(p);
+                const uint32_t* cells = defer_cells.as<uint32_t>();
+                if (indexed) { if (hp) k_deferred_h<true, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<true, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
+                else { if (hp) k_deferred_h<false, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<false, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
+            }
+        } else {
+            // --- pre-current ---
+            if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            // --- core H (+UPML) ---
+            dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
+            if (indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, stream>>>(g, ps); }
+            else { if (hp) k_curr<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<false, false><<<cg, cb, 0, stream>>>(g, ps); }
+        }
+        // --- post-current (on the updated H) ---
+        if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C1, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
+        if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, false, C1);
         // --- after the step ---
-        if (nf_on) k_nf2ff<<<blocks(nf.np, T), T, 0, stream>>>(V, C, st, k, nf);
+        if (nf_on) k_nf2ff<<<blocks(nf.np, T), T, 0, stream>>>(V1, C1, st, k, nf);
         if (ring_on)
-            k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V, C, st, k, ring_idx.as<uint32_t>(), ring_n, ring_interval,
+            k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V1, C1, st, k, ring_idx.as<uint32_t>(), ring_n, ring_interval,
                                                                   ring_q0, ring_max, ring.as<float>());
+    }
+
+    template <int CPT, int TY, bool VEC>
+    void launch_fused_t(int p) {
+        const FusedGrid fg = fused_grid(p);
+        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
+        dim3 b(32, TY + 1), g(blocks(Nz, 32 * CPT), blocks(Ny, TY), blocks(Nx, xchunk));
+        const bool hp = !pml.empty();
+        if (indexed) { if (hp) k_fused<true, true, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<true, false, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); }
+        else { if (hp) k_fused<false, true, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<false, false, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); }
+    }
+    void launch_fused(int p) {
+        const bool vec2 = (Nz % 2) == 0, vec4 = (Nz % 4) == 0;
+        if (cpt >= 4 && vec4) launch_fused_t<4, 8, true>(p);
+        else if (cpt >= 2 && vec2) launch_fused_t<2, 8, true>(p);
+        else if (cpt >= 2) launch_fused_t<2, 8, false>(p);
+        else launch_fused_t<1, 8, false>(p);
     }
 
     PointSources point_dev(const PointSet& p, const DevBuf& sig, uint32_t len, uint32_t period) const {
@@ -340,7 +461,7 @@ struct efs_engine {
         return RlcDev{rlc_n, rlc_groups, rlc_gtarget.as<uint32_t>(), rlc_goff.as<uint32_t>(), rlc_type.as<uint32_t>(),
                       rlc_p.as<float>(), rlc_vdn.as<float>(), rlc_jn.as<float>(), rlc_vil.as<float>()};
     }
-    void launch_pbc(const PbcAxis& a, bool isVolt) {
+    void launch_pbc(const PbcAxis& a, bool isVolt, float* F) {
         const uint32_t nl[3] = {Nx, Ny, Nz};
         PbcDev p;
         p.axis = a.axis; p.volt = isVolt ? 1 : 0;
@@ -350,7 +471,6 @@ struct efs_engine {
         p.src = isVolt ? nl[a.axis] - 2 : 0; p.dst = isVolt ? 0 : nl[a.axis] - 2;
         p.Nx = Nx; p.Ny = Ny; p.Nz = Nz; p.cosP = a.c; p.sinP = a.s;
         p.imag = pbc_imag.as<float>() + a.imag_off;
-        float* F = isVolt ? volt.as<float>() : curr.as<float>();
         dim3 b(16, 16), gr(blocks(p.b0, 16), blocks(p.b1, 16));
         if (p.b0 && p.b1) k_pbc<<<gr, b, 0, stream>>>(F, p);
     }
@@ -361,22 +481,26 @@ struct efs_engine {
         const uint32_t CH = 64;   // steps per captured graph
         while (n > 0) {
             uint32_t m = std::min(n, CH);
-            cudaGraphExec_t ge = graph_for(m);
+            cudaGraphExec_t ge = graph_for(m, cur);
             ck(cudaGraphLaunch(ge, stream), "cudaGraphLaunch");
             numTS += m;
+            if (fused && (m & 1)) cur ^= 1;
             n -= m;
         }
         ck(cudaGetLastError(), "iterate");
     }
 
-    cudaGraphExec_t graph_for(uint32_t m) {
-        auto it = graphs.find(m);
+    // graph of m steps starting from parity p (the buffers alternate each step)
+    cudaGraphExec_t graph_for(uint32_t m, int p) {
+        const uint32_t key = m * 2 + (uint32_t)p;
+        auto it = graphs.find(key);
         if (it != graphs.end()) return it->second;
-        if (graphs.size() > 8) drop_graphs();
+        if (graphs.size() > 12) drop_graphs();
         cudaGraph_t graph;
         ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "BeginCapture");
         try {
-            for (uint32_t k = 0; k < m; ++k) enqueue_step(k);
+            int q = p;
+            for (uint32_t k = 0; k < m; ++k) { enqueue_step(k, q); q = pnext(q); }
             k_advance<<<1, 1, 0, stream>>>(state.as<StepState>(), m);
         } catch (...) {
             cudaStreamEndCapture(stream, &graph);
@@ -387,7 +511,7 @@ struct efs_engine {
         cudaError_t err = cudaGraphInstantiate(&ge, graph, 0);
         cudaGraphDestroy(graph);
         ck(err, "cudaGraphInstantiate");
-        graphs[m] = ge;
+        graphs[key] = ge;
         return ge;
     }
 
@@ -441,8 +565,23 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     e->ade_v = efs_engine::AdeSide(); e->ade_c = efs_engine::AdeSide();
     e->gd_n = 0;
     e->Nx = dims[0]; e->Ny = dims[1]; e->Nz = dims[2]; e->N = N;
+    e->h_exc_targets.clear(); e->h_tfsf_v_targets.clear(); e->h_mur_apply.clear(); e->h_rlc_series.clear();
+    e->defer_n = 0;
+    // core path and fused-kernel shape: EFS_CORE=split selects separate E/H sweeps
+    const char* core = getenv("EFS_CORE");
+    e->fused = !(core && std::string(core) == "split");
+    if (const char* s = getenv("EFS_XCHUNK")) e->xchunk = std::max(1, atoi(s));
+    if (const char* s = getenv("EFS_CPT")) e->cpt = std::max(1, atoi(s));
+    e->cur = 0;
     e->alloc(e->volt, 3 * N * sizeof(float));
     e->alloc(e->curr, 3 * N * sizeof(float));
+    if (e->fused) {
+        e->alloc(e->volt_b, 3 * N * sizeof(float));
+        e->alloc(e->curr_b, 3 * N * sizeof(float));
+    } else {
+        e->volt_b.reset();
+        e->curr_b.reset();
+    }
     e->alloc(e->state, sizeof(StepState));
     e->numTS = 0;
     e->hstate = StepState{};
@@ -577,6 +716,7 @@ efs_status efs_configure_excitation(efs_engine* e, const float* signal, uint32_t
         std::vector<float> a(count);
         for (uint32_t i = 0; i < count; ++i) { d[i] = delay[perm[i]]; a[i] = amp[perm[i]]; }
         e->upload(e->exc_target, ut); e->upload(e->exc_off, off);
+        e->h_exc_targets = ut;
         e->upload(e->exc_delay, d); e->upload(e->exc_amp, a);
         e->upload(e->exc_signal, signal, L);
         e->exc_groups = (uint32_t)ut.size(); e->exc_len = L; e->exc_period = period;
@@ -605,7 +745,21 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
             e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
             e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
             e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
+            if (e->fused) { e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4); }
             out.push_back(std::move(R));
+        }
+        // the per-cell UPML chain keeps at most PML_MAX_OVERLAP regions in registers:
+        // test every corner formed by region bounds (the overlap count is maximal at one)
+        if (count > (uint32_t)PML_MAX_OVERLAP) {
+            std::vector<uint32_t> cx[3];
+            for (auto& R : out)
+                for (int d = 0; d < 3; ++d) cx[d].push_back(R->s[d]);
+            for (uint32_t a : cx[0]) for (uint32_t b : cx[1]) for (uint32_t c : cx[2]) {
+                int k = 0;
+                for (auto& R : out)
+                    k += (a - R->s[0]) < R->n[0] && (b - R->s[1]) < R->n[1] && (c - R->s[2]) < R->n[2];
+                if (k > PML_MAX_OVERLAP) fail(EFS_ERR_RANGE, "more than 4 UPML regions overlap at one cell");
+            }
         }
         e->pml = std::move(out);
         e->dirty();
@@ -633,6 +787,7 @@ efs_status efs_configure_mur(efs_engine* e, const float* coeff, const uint32_t* 
         e->upload(e->mur_coeff, coeff, n);
         e->upload(e->mur_shifted, shifted, n);
         e->upload(e->mur_apply_target, at); e->upload(e->mur_apply_src, as);
+        e->h_mur_apply = at;
         e->alloc(e->mur_saved, (size_t)n * 4);
         e->mur_n = n; e->mur_napply = (uint32_t)order.size();
         e->mur_on = n > 0;
@@ -660,6 +815,8 @@ efs_status efs_configure_tfsf(efs_engine* e, const float* signal, uint32_t L, ui
         if (!signal || L == 0) fail(EFS_ERR_INVALID, "TFSF signal must be non-empty");
         if ((nv && !vp) || (nc && !cp)) fail(EFS_ERR_INVALID, "TFSF point arrays must be non-null");
         build_points(e, e->tfsf_v, vp, nv);
+        e->h_tfsf_v_targets.clear();
+        for (uint32_t i = 0; i < nv; ++i) e->h_tfsf_v_targets.push_back(vp[i].field_idx);
         build_points(e, e->tfsf_c, cp, nc);
         e->upload(e->tfsf_signal, signal, L);
         e->tfsf_len = L; e->tfsf_period = period;
@@ -725,6 +882,8 @@ efs_status efs_configure_rlc(efs_engine* e, uint32_t n, const efs_rlc_element* e
         std::vector<float> p2(9 * (size_t)n);
         for (uint32_t i = 0; i < n; ++i) { type2[i] = type[perm[i]]; memcpy(&p2[9 * (size_t)i], &p[9 * (size_t)perm[i]], 36); }
         e->upload(e->rlc_gtarget, ut); e->upload(e->rlc_goff, goff);
+        e->h_rlc_series.clear();
+        for (uint32_t i = 0; i < n; ++i) if (el[i].type_flag == 1) e->h_rlc_series.push_back(tgt[i]);
         e->upload(e->rlc_type, type2); e->upload(e->rlc_p, p2);
         e->alloc(e->rlc_vdn, 3 * (size_t)n * 4); e->alloc(e->rlc_jn, 3 * (size_t)n * 4); e->alloc(e->rlc_vil, (size_t)n * 4);
         e->rlc_n = n; e->rlc_groups = (uint32_t)ut.size();
@@ -848,7 +1007,7 @@ efs_status efs_read_probe_gather(efs_engine* e, float* out, size_t len) {
         e->need_init();
         if (!e->gd_n) fail(EFS_ERR_STATE, "probe gather not configured");
         if (!out || len < 2 * (size_t)e->gd_n) fail(EFS_ERR_INVALID, "output buffer too small");
-        k_gather<<<blocks(e->gd_n, 64), 64, 0, e->stream>>>(e->volt.as<float>(), e->curr.as<float>(), e->gd_idx.as<uint32_t>(),
+        k_gather<<<blocks(e->gd_n, 64), 64, 0, e->stream>>>(e->vcur(), e->ccur(), e->gd_idx.as<uint32_t>(),
                                                              e->gd_n, e->gd_out.as<float>());
         ck(cudaGetLastError(), "gather");
         ck(cudaMemcpyAsync(out, e->gd_out.p, 2 * (size_t)e->gd_n * 4, cudaMemcpyDeviceToHost, e->stream), "read gather");
@@ -987,7 +1146,7 @@ static void energy_launch(efs_engine* e, int slot) {
     if (e->Nx < 2 || e->Ny < 2 || e->Nz < 2) {
         ck(cudaMemsetAsync(res, 0, sizeof(double), e->stream), "memset");
     } else {
-        k_energy<<<1024, 256, 0, e->stream>>>(e->volt.as<float>(), e->curr.as<float>(), e->Nx, e->Ny, e->Nz, e->en_partial.as<double>());
+        k_energy<<<1024, 256, 0, e->stream>>>(e->vcur(), e->ccur(), e->Nx, e->Ny, e->Nz, e->en_partial.as<double>());
         k_energy_final<<<1, 1024, 0, e->stream>>>(e->en_partial.as<double>(), 1024, res);
     }
     ck(cudaGetLastError(), "energy");
@@ -1034,8 +1193,8 @@ efs_status efs_flush_energy(efs_engine* e, double* out) {
 efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
     return guard(e, [&] {
         e->need_init();
-        if (v) ck(cudaMemcpyAsync(v, e->volt.p, 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read volt");
-        if (c) ck(cudaMemcpyAsync(c, e->curr.p, 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read curr");
+        if (v) ck(cudaMemcpyAsync(v, e->vcur(), 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read volt");
+        if (c) ck(cudaMemcpyAsync(c, e->ccur(), 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read curr");
         ck(cudaStreamSynchronize(e->stream), "sync");
     });
 }
@@ -1043,16 +1202,17 @@ efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
 efs_status efs_set_fields(efs_engine* e, const float* v, const float* c) {
     return guard(e, [&] {
         e->need_init();
-        if (v) ck(cudaMemcpyAsync(e->volt.p, v, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write volt");
-        if (c) ck(cudaMemcpyAsync(e->curr.p, c, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write curr");
+        if (v) ck(cudaMemcpyAsync(e->vcur(), v, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write volt");
+        if (c) ck(cudaMemcpyAsync(e->ccur(), c, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write curr");
         ck(cudaStreamSynchronize(e->stream), "sync");
     });
 }
 
 // state blob: magic, version, numTS, nbuf, then per buffer (bytes, data)
 static std::vector<DevBuf*> state_buffers(efs_engine* e) {
-    std::vector<DevBuf*> b = {&e->volt, &e->curr};
-    for (auto& r : e->pml) { b.push_back(&r->vflux); b.push_back(&r->cflux); }
+    const int p = e->cur;
+    std::vector<DevBuf*> b = {p ? &e->volt_b : &e->volt, p ? &e->curr_b : &e->curr};
+    for (auto& r : e->pml) { b.push_back(p && r->vflux_b.p ? &r->vflux_b : &r->vflux); b.push_back(p && r->cflux_b.p ? &r->cflux_b : &r->cflux); }
     if (e->mur_on) b.push_back(&e->mur_saved);
     for (auto* s : {&e->ade_v, &e->ade_c}) if (s->n) { b.push_back(&s->state); b.push_back(&s->lor); }
     if (e->rlc_on) { b.push_back(&e->rlc_vdn); b.push_back(&e->rlc_jn); b.push_back(&e->rlc_vil); }
@@ -1121,7 +1281,9 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
         const DevBuf* b = nullptr;
         size_t n = 0;
         if ((s == "pml_volt_flux" || s == "pml_curr_flux") && arg < e->pml.size()) {
-            b = s == "pml_volt_flux" ? &e->pml[arg]->vflux : &e->pml[arg]->cflux;
+            const int p = e->cur;
+            auto& R = *e->pml[arg];
+            b = s == "pml_volt_flux" ? (p && R.vflux_b.p ? &R.vflux_b : &R.vflux) : (p && R.cflux_b.p ? &R.cflux_b : &R.cflux);
             n = e->pml[arg]->total;
         } else if (s == "mur_saved" && e->mur_on) { b = &e->mur_saved; n = e->mur_n; }
         else if (s == "ade_volt") { b = &e->ade_v.state; n = e->ade_v.n; }
@@ -1161,6 +1323,21 @@ efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms) {
         dim3 cb(CORE_BZ, CORE_BY), cg(blocks(e->Nz, CORE_BZ), blocks(e->Ny, CORE_BY), blocks(e->Nx, CORE_TX));
         cudaEvent_t ev[3];
         for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+        if (e->fused) {
+            // the fused kernel reads parity cur and writes the other one; repeated
+            // launches redo the same step, which is what is timed
+            ck(cudaEventRecord(ev[0], e->stream), "record");
+            for (uint32_t i = 0; i < reps; ++i) e->launch_fused(e->cur);
+            ck(cudaEventRecord(ev[1], e->stream), "record");
+            ck(cudaEventSynchronize(ev[1]), "sync");
+            ck(cudaGetLastError(), "fused launch");
+            float a = 0;
+            cudaEventElapsedTime(&a, ev[0], ev[1]);
+            for (auto& x : ev) cudaEventDestroy(x);
+            ms[0] = a / reps;
+            ms[1] = 0.f;
+            return;
+        }
         auto volt = [&] {
             if (e->indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, e->stream>>>(g, ps); }
             else { if (hp) k_volt<false, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, e->stream>>>(g, ps); }
@@ -1188,7 +1365,8 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
     return guard(e, [&] {
         e->need_init();
         if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
-        uint32_t k = 2;                                        // core E and H
+        e->build_plan();
+        uint32_t k = e->fused ? 1 + (e->defer_n > 0) : 2;      // core: fused (+ deferred H) or E and H
         k += e->ss_on + (e->ade_v.n > 0) + (e->ade_c.n > 0) + 3 * e->mur_on + 2 * e->rlc_on;
         k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
         k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;
@@ -1200,10 +1378,10 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
 efs_status efs_device_bytes(const efs_engine* e, size_t* out) {
     if (!e || !out) return EFS_ERR_INVALID;
     size_t t = 0;
-    const DevBuf* all[] = {&e->volt, &e->curr, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
+    const DevBuf* all[] = {&e->volt, &e->curr, &e->volt_b, &e->curr_b, &e->defer_bits, &e->defer_cells, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
     for (auto* b : all) t += b->bytes;
     for (auto& r : e->pml) {
-        const DevBuf* rb[] = {&r->vv, &r->vvfo, &r->vvfn, &r->ii, &r->iifo, &r->iifn, &r->vflux, &r->cflux};
+        const DevBuf* rb[] = {&r->vv, &r->vvfo, &r->vvfn, &r->ii, &r->iifo, &r->iifn, &r->vflux, &r->cflux, &r->vflux_b, &r->cflux_b};
         for (auto* b : rb) t += b->bytes;
     }
     t += e->nf_E.bytes + e->nf_H.bytes + e->ring.bytes;

@@ -18,6 +18,25 @@ from oracle.oracle import OracleEngine, far_field
 
 pytestmark = pytest.mark.gpu
 
+# Core-update paths: the single-pass fused kernel in several tile shapes
+# (cells per thread along z, x-planes per block; small chunks put block seams
+# inside the test grids) and the separate E/H sweeps.
+CORES = {
+    "fused": {},
+    "fused_cpt4_x3": {"EFS_CPT": "4", "EFS_XCHUNK": "3"},
+    "fused_cpt1_x5": {"EFS_CPT": "1", "EFS_XCHUNK": "5"},
+    "split": {"EFS_CORE": "split"},
+}
+
+
+@pytest.fixture(autouse=True, params=list(CORES))
+def core_path(request, monkeypatch):
+    for k in ("EFS_CORE", "EFS_CPT", "EFS_XCHUNK"):
+        monkeypatch.delenv(k, raising=False)
+    for k, v in CORES[request.param].items():
+        monkeypatch.setenv(k, v)
+    return request.param
+
 
 def rand_coeffs(N, seed, pec_frac=0.05):
     Nx, Ny, Nz = N
