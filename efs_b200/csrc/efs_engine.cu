@@ -427,21 +427,19 @@ struct efs_engine {
                                                                   ring_q0, ring_max, ring.as<float>());
     }
 
-    template <int CPT, int TY, bool VEC>
+    template <int CPT, int TY>
     void launch_fused_t(int p) {
         const FusedGrid fg = fused_grid(p);
         const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
         dim3 b(32, TY + 1), g(blocks(Nz, 32 * CPT), blocks(Ny, TY), blocks(Nx, xchunk));
         const bool hp = !pml.empty();
-        if (indexed) { if (hp) k_fused<true, true, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<true, false, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); }
-        else { if (hp) k_fused<false, true, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<false, false, CPT, TY, VEC><<<g, b, 0, stream>>>(fg, ps, pn); }
+        if (indexed) { if (hp) k_fused<true, true, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<true, false, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); }
+        else { if (hp) k_fused<false, true, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<false, false, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); }
     }
     void launch_fused(int p) {
-        const bool vec2 = (Nz % 2) == 0, vec4 = (Nz % 4) == 0;
-        if (cpt >= 4 && vec4) launch_fused_t<4, 8, true>(p);
-        else if (cpt >= 2 && vec2) launch_fused_t<2, 8, true>(p);
-        else if (cpt >= 2) launch_fused_t<2, 8, false>(p);
-        else launch_fused_t<1, 8, false>(p);
+        if (cpt >= 4) launch_fused_t<4, 8>(p);
+        else if (cpt >= 2) launch_fused_t<2, 8>(p);
+        else launch_fused_t<1, 8>(p);
     }
 
     PointSources point_dev(const PointSet& p, const DevBuf& sig, uint32_t len, uint32_t period) const {

@@ -83,29 +83,20 @@ __device__ __forceinline__ void coeffs_f(const FusedGrid& g, size_t c, uint32_t 
     }
 }
 
-template <int CPT, bool VEC>
-__device__ __forceinline__ void load_cells(const float* __restrict__ p, bool ok[CPT], float out[CPT]) {
-    if (VEC && ok[CPT - 1]) {   // ok[] is a prefix: the last cell valid means all are
-        if (CPT == 4) { float4 v = __ldg(reinterpret_cast<const float4*>(p)); out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w; return; }
-        if (CPT == 2) { float2 v = __ldg(reinterpret_cast<const float2*>(p)); out[0] = v.x; out[1] = v.y; return; }
-    }
+// A lane's cell k sits at z = z0 + k*32 + lane: every access is coalesced
+// across the warp and conflict-free in shared memory.
+template <int CPT>
+__device__ __forceinline__ void load_cells(const float* __restrict__ p, const bool ok[CPT], float out[CPT]) {
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) out[k] = ok[k] ? __ldg(p + k) : 0.f;
+    for (int k = 0; k < CPT; ++k) out[k] = ok[k] ? __ldg(p + 32 * k) : 0.f;
 }
-template <int CPT, bool VEC>
-__device__ __forceinline__ void store_cells(float* __restrict__ p, bool ok[CPT], const float v[CPT]) {
-    bool all = true;
+template <int CPT>
+__device__ __forceinline__ void store_cells(float* __restrict__ p, const bool ok[CPT], const float v[CPT]) {
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) all = all && ok[k];
-    if (VEC && all) {
-        if (CPT == 4) { *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]); return; }
-        if (CPT == 2) { *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]); return; }
-    }
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) if (ok[k]) p[k] = v[k];
+    for (int k = 0; k < CPT; ++k) if (ok[k]) p[32 * k] = v[k];
 }
 
-template <bool IDX, bool PML, int CPT, int TY, bool VEC>
+template <bool IDX, bool PML, int CPT, int TY>
 __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, const PmlSet ps, const PmlSet pn) {
     constexpr int TZ = 32 * CPT;
     constexpr int W = TZ + 2;                    // column j <-> z = z0 - 1 + j
@@ -114,7 +105,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
     const int lane = threadIdx.x, ty = threadIdx.y;
     const uint32_t z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY;
     const uint32_t y = y0 + ty;
-    const uint32_t zc = z0 + lane * CPT;
+    const uint32_t zc = z0 + lane;             // cell k: z = zc + 32*k
     const bool rowIn = y < g.Ny;
     const bool own_row = ty < TY;
     const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
@@ -126,7 +117,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
     const uint32_t ze = z0 + TZ;
     bool ok[CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) ok[k] = rowIn && (zc + k < g.Nz);
+    for (int k = 0; k < CPT; ++k) ok[k] = rowIn && (zc + 32 * k < g.Nz);
     const uint32_t ym = y0 > 0 ? y0 - 1 : y0;      // low y halo row (self at y = 0)
     const uint32_t zm = z0 > 0 ? z0 - 1 : z0;      // low z halo column (self at z = 0)
 
@@ -137,7 +128,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
             float t[CPT];
-            load_cells<CPT, VEC>(g.H0 + n * N + b, ok, t);
+            load_cells<CPT>(g.H0 + n * N + b, ok, t);
 #pragma unroll
             for (int k = 0; k < CPT; ++k) hp[k][n] = t[k];
             if (extra) hpe[n] = __ldg(g.H0 + n * N + (size_t)(xs - 1) * NyNz + (size_t)y * Nz + ze);
@@ -153,9 +144,9 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
             float t[CPT];
-            load_cells<CPT, VEC>(g.H0 + n * N + b, ok, t);
+            load_cells<CPT>(g.H0 + n * N + b, ok, t);
 #pragma unroll
-            for (int k = 0; k < CPT; ++k) { hc[k][n] = t[k]; sH[n][ty + 1][1 + lane * CPT + k] = t[k]; }
+            for (int k = 0; k < CPT; ++k) { hc[k][n] = t[k]; sH[n][ty + 1][1 + 32 * k + lane] = t[k]; }
             if (extra) { hce[n] = __ldg(g.H0 + n * N + (size_t)x * NyNz + (size_t)y * Nz + ze); sH[n][ty + 1][TZ + 1] = hce[n]; }
         }
         if (ty == 0) {
@@ -163,13 +154,13 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
             const size_t bm = (size_t)x * NyNz + (size_t)ym * Nz + zc;
             bool okm[CPT];
 #pragma unroll
-            for (int k = 0; k < CPT; ++k) okm[k] = rin && (zc + k < g.Nz);
+            for (int k = 0; k < CPT; ++k) okm[k] = rin && (zc + 32 * k < g.Nz);
 #pragma unroll
             for (int n = 0; n < 3; n += 2) {     // Hx, Hz at y-1
                 float t[CPT];
-                load_cells<CPT, VEC>(g.H0 + n * N + bm, okm, t);
+                load_cells<CPT>(g.H0 + n * N + bm, okm, t);
 #pragma unroll
-                for (int k = 0; k < CPT; ++k) sH[n][0][1 + lane * CPT + k] = t[k];
+                for (int k = 0; k < CPT; ++k) sH[n][0][1 + 32 * k + lane] = t[k];
                 if (lane == 31 && rin && ze < g.Nz) sH[n][0][TZ + 1] = __ldg(g.H0 + n * N + (size_t)x * NyNz + (size_t)ym * Nz + ze);
             }
         }
@@ -183,7 +174,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
             float t[CPT];
-            load_cells<CPT, VEC>(g.V0 + n * N + b, ok, t);
+            load_cells<CPT>(g.V0 + n * N + b, ok, t);
 #pragma unroll
             for (int k = 0; k < CPT; ++k) eo[k][n] = t[k];
             if (extra) eoe[n] = __ldg(g.V0 + n * N + (size_t)x * NyNz + (size_t)y * Nz + ze);
@@ -191,7 +182,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
         uint32_t matc[CPT], mate = 0;
         if (IDX) {
 #pragma unroll
-            for (int k = 0; k < CPT; ++k) matc[k] = ok[k] ? __ldg(g.mat + (b + k) - 0) : 0u;
+            for (int k = 0; k < CPT; ++k) matc[k] = ok[k] ? __ldg(g.mat + b + 32 * k) : 0u;
             if (extra) mate = __ldg(g.mat + (size_t)x * NyNz + (size_t)y * Nz + ze);
         } else {
 #pragma unroll
@@ -203,8 +194,8 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
         float en[CPT][3];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int j = 1 + lane * CPT + k;
-            const uint32_t z = zc + k;
+            const int j = 1 + 32 * k + lane;
+            const uint32_t z = zc + 32 * k;
             if (!ok[k]) { en[k][0] = en[k][1] = en[k][2] = 0.f; }
             else {
                 const float hy_xm = x0self ? hc[k][1] : hp[k][1], hz_xm = x0self ? hc[k][2] : hp[k][2];
@@ -212,7 +203,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
                 const float cy = curl4(hc[k][0], sH[0][ty + 1][j - 1], hc[k][2], hz_xm);
                 const float cz = curl4(hc[k][1], hy_xm, hc[k][0], sH[0][ty][j]);
                 float kk[6];
-                coeffs_f<IDX>(g, b + k, matc[k], 0, kk);
+                coeffs_f<IDX>(g, b + 32 * k, matc[k], 0, kk);
                 if (PML) {
                     const bool wr = own_row && x < xe;
                     en[k][0] = pml_chain_pp<true>(ps, pn, x, y, z, 0, eo[k][0], true, kk[0], kk[3], cx, wr);
@@ -257,7 +248,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
                 float t[CPT];
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) t[k] = en[k][n];
-                store_cells<CPT, VEC>(g.V1 + n * N + b, ok, t);
+                store_cells<CPT>(g.V1 + n * N + b, ok, t);
             }
         }
         __syncthreads();
@@ -269,11 +260,11 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
             bool wr[CPT];
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                const int j = 1 + lane * CPT + k;
-                const uint32_t z = zc + k;
+                const int j = 1 + 32 * k + lane;
+                const uint32_t z = zc + 32 * k;
                 wr[k] = ok[k];
                 if (ok[k] && g.defer) {
-                    const size_t cm = bm1 + k;
+                    const size_t cm = bm1 + 32 * k;
                     if ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) wr[k] = false;
                 }
                 hn[k][0] = hn[k][1] = hn[k][2] = 0.f;
@@ -287,7 +278,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
                     cz = curl4(ey, en[k][1], ex, sE[pe][0][ty + 1][j]);
                 }
                 float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                if (core) coeffs_f<IDX>(g, bm1 + k, matp[k], 6, kk);
+                if (core) coeffs_f<IDX>(g, bm1 + 32 * k, matp[k], 6, kk);
                 if (PML) {
                     hn[k][0] = pml_chain_pp<false>(ps, pn, x - 1, y, z, 0, hp[k][0], core, kk[0], kk[3], cx, true);
                     hn[k][1] = pml_chain_pp<false>(ps, pn, x - 1, y, z, 1, hp[k][1], core, kk[1], kk[4], cy, true);
@@ -305,7 +296,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
                 float t[CPT];
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) t[k] = hn[k][n];
-                store_cells<CPT, VEC>(g.H1 + n * N + bm1, wr, t);
+                store_cells<CPT>(g.H1 + n * N + bm1, wr, t);
             }
         }
         // ---- rotate
@@ -325,12 +316,12 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
         for (int k = 0; k < CPT; ++k) {
             wr[k] = ok[k];
             if (ok[k] && g.defer) {
-                const size_t cm = bl + k;
+                const size_t cm = bl + 32 * k;
                 if ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) wr[k] = false;
             }
 #pragma unroll
             for (int n = 0; n < 3; ++n)
-                hn[k][n] = (PML && wr[k]) ? pml_chain_pp<false>(ps, pn, g.Nx - 1, y, zc + k, n, hp[k][n], false, 0.f, 0.f, 0.f, true)
+                hn[k][n] = (PML && wr[k]) ? pml_chain_pp<false>(ps, pn, g.Nx - 1, y, zc + 32 * k, n, hp[k][n], false, 0.f, 0.f, 0.f, true)
                                           : hp[k][n];
         }
 #pragma unroll
@@ -338,7 +329,7 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
             float t[CPT];
 #pragma unroll
             for (int k = 0; k < CPT; ++k) t[k] = hn[k][n];
-            store_cells<CPT, VEC>(g.H1 + n * N + bl, wr, t);
+            store_cells<CPT>(g.H1 + n * N + bl, wr, t);
         }
     }
 }

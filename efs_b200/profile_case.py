@@ -1,0 +1,41 @@
+"""Small, self-terminating run of the headline workload for profilers.
+
+    python -m efs_b200.profile_case --n 256 --steps 4
+
+builds workloads.large_plain(n) (n^3 lines: same features as the benchmark),
+configures the CUDA engine and runs `steps` timesteps, printing the mean
+device time per timestep.  Sized by --n so a profiler capture stays small.
+"""
+import argparse
+import time
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=2)
+    args = ap.parse_args()
+    from efs_b200.build import build
+    build()
+    from efs_b200 import workloads
+    from efs_b200.engine import CudaEngine
+    job = workloads.large_plain(args.n)
+    eng = CudaEngine()
+    if not eng.initGPU():
+        raise SystemExit("no CUDA device")
+    workloads.configure(eng, dict(job, probes=[]))
+    eng.iterate(args.warmup)
+    eng.sync()
+    t = time.perf_counter()
+    eng.iterate(args.steps)
+    eng.sync()
+    dt = (time.perf_counter() - t) / max(1, args.steps)
+    N = args.n ** 3
+    print("n=%d steps=%d  %.3f ms/timestep  %.1f MCells/s  kernels/step=%d" %
+          (args.n, args.steps, dt * 1e3, N / dt / 1e6, eng.kernelsPerStep()))
+    eng.destroy()
+
+
+if __name__ == "__main__":
+    main()
