@@ -89,7 +89,8 @@ struct efs_engine {
     bool fused = true;          // single-pass E+H kernel (else separate E and H sweeps)
     int cur = 0;                // parity holding the current fields
     uint32_t xchunk = 64;       // x-planes per block of the fused kernel
-    int cpt = 2;                // z cells per thread of the fused kernel
+    int cpt = 1;                // z cells per thread of the fused kernel (1 or 2)
+    int ty_rows = 8;            // y rows per tile of the fused kernel (8 or 16)
     DevBuf defer_bits, defer_cells;
     uint32_t defer_n = 0;
     std::vector<uint32_t> h_exc_targets, h_tfsf_v_targets, h_mur_apply, h_rlc_series;
@@ -427,19 +428,28 @@ struct efs_engine {
                                                                   ring_q0, ring_max, ring.as<float>());
     }
 
+    template <bool IDX, bool PML, int CPT, int TY>
+    void launch_fused_k(dim3 g, dim3 b, const FusedGrid& fg, const PmlSet& ps, const PmlSet& pn) {
+        const size_t sm = sizeof(FusedSmem<CPT, TY>);
+        static bool attr_set = false;   // per instantiation; the attribute is per kernel, all devices alike
+        if (!attr_set) {
+            ck(cudaFuncSetAttribute(k_fused<IDX, PML, CPT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attr");
+            attr_set = true;
+        }
+        k_fused<IDX, PML, CPT, TY><<<g, b, sm, stream>>>(fg, ps, pn);
+    }
     template <int CPT, int TY>
     void launch_fused_t(int p) {
         const FusedGrid fg = fused_grid(p);
         const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
         dim3 b(32, TY + 1), g(blocks(Nz, 32 * CPT), blocks(Ny, TY), blocks(Nx, xchunk));
         const bool hp = !pml.empty();
-        if (indexed) { if (hp) k_fused<true, true, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<true, false, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); }
-        else { if (hp) k_fused<false, true, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused<false, false, CPT, TY><<<g, b, 0, stream>>>(fg, ps, pn); }
+        if (indexed) { if (hp) launch_fused_k<true, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<true, false, CPT, TY>(g, b, fg, ps, pn); }
+        else { if (hp) launch_fused_k<false, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<false, false, CPT, TY>(g, b, fg, ps, pn); }
     }
     void launch_fused(int p) {
-        if (cpt >= 4) launch_fused_t<4, 8>(p);
-        else if (cpt >= 2) launch_fused_t<2, 8>(p);
-        else launch_fused_t<1, 8>(p);
+        if (cpt >= 2) { if (ty_rows >= 16) launch_fused_t<2, 16>(p); else launch_fused_t<2, 8>(p); }
+        else { if (ty_rows >= 16) launch_fused_t<1, 16>(p); else launch_fused_t<1, 8>(p); }
     }
 
     PointSources point_dev(const PointSet& p, const DevBuf& sig, uint32_t len, uint32_t period) const {
@@ -570,6 +580,7 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     e->fused = !(core && std::string(core) == "split");
     if (const char* s = getenv("EFS_XCHUNK")) e->xchunk = std::max(1, atoi(s));
     if (const char* s = getenv("EFS_CPT")) e->cpt = std::max(1, atoi(s));
+    if (const char* s = getenv("EFS_TY")) e->ty_rows = std::max(8, atoi(s));
     e->cur = 0;
     e->alloc(e->volt, 3 * N * sizeof(float));
     e->alloc(e->curr, 3 * N * sizeof(float));

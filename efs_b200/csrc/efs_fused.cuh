@@ -38,13 +38,16 @@ struct FusedGrid {
 
 // UPML chain with separate old/new flux buffers; up to PML_MAX_OVERLAP regions per cell.
 template <bool VOLT>
-__device__ __forceinline__ float pml_chain_pp(const PmlSet& ps, const PmlSet& pn, uint32_t x, uint32_t y, uint32_t z,
-                                              uint32_t n, float vold, bool core, float cv, float ci, float curl, bool write) {
+__device__ __forceinline__ float pml_chain_pp(const PmlSet& ps, const PmlSet& pn, uint32_t mask, uint32_t x, uint32_t y,
+                                              uint32_t z, uint32_t n, float vold, bool core, float cv, float ci, float curl,
+                                              bool write) {
     int reg[PML_MAX_OVERLAP];
     size_t pp[PML_MAX_OVERLAP];
     int cnt = 0;
-    for (int r = 0; r < ps.count; ++r)
+    for (uint32_t m = mask; m; m &= m - 1) {
+        const int r = __ffs(m) - 1;
         if (in_region(ps.r[r], x, y, z) && cnt < PML_MAX_OVERLAP) { reg[cnt] = r; pp[cnt] = region_p(ps.r[r], n, x, y, z); ++cnt; }
+    }
     if (cnt == 0) return core ? upd(vold, cv, ci, curl) : vold;
     float fh[PML_MAX_OVERLAP];
     float v = vold;
@@ -96,240 +99,268 @@ __device__ __forceinline__ void store_cells(float* __restrict__ p, const bool ok
     for (int k = 0; k < CPT; ++k) if (ok[k]) p[32 * k] = v[k];
 }
 
+
+// cp.async of one float into shared memory; `valid` false zero-fills without reading
+__device__ __forceinline__ void cp4(float* smem, const float* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 4 : 0));
+}
+__device__ __forceinline__ void cp4u(uint32_t* smem, const uint32_t* gmem, bool valid) {
+    cp4(reinterpret_cast<float*>(smem), reinterpret_cast<const float*>(gmem), valid);
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int NW>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NW)); }
+
+template <int CPT, int TY>
+struct FusedSmem {
+    static constexpr int TZ = 32 * CPT;
+    static constexpr int W = TZ + 2;          // column j <-> z = z0 - 1 + j
+    float H[2][3][TY + 2][W];                 // H_old of a plane, rows y0-1 .. y0+TY (double-buffered)
+    float E[2][3][TY + 1][W];                 // E_old of a plane, rows y0 .. y0+TY
+    uint32_t M[2][TY + 1][W];                 // material rows
+    float En[2][3][TY + 1][W];                // E_new of planes x-1, x
+};
+
+// Stage plane x of the tile (H with low halos, E_old, material) into buffer b.
+template <bool IDX, int CPT, int TY>
+__device__ __forceinline__ void stage_plane(FusedSmem<CPT, TY>& S, int b, const FusedGrid& g, uint32_t x, uint32_t y0,
+                                            uint32_t z0, int lane, int ty) {
+    constexpr int TZ = 32 * CPT;
+    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
+    const uint32_t y = y0 + ty;
+    const bool rowIn = y < g.Ny;
+    const size_t base = (size_t)x * NyNz + (size_t)(rowIn ? y : 0) * Nz;
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const uint32_t z = z0 + lane + 32 * k;
+        const bool ok = rowIn && z < g.Nz;
+        const size_t c = base + (ok ? z : 0);
+        const int j = 1 + 32 * k + lane;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            cp4(&S.H[b][n][ty + 1][j], g.H0 + n * N + c, ok);
+            cp4(&S.E[b][n][ty][j], g.V0 + n * N + c, ok);
+        }
+        if (IDX) cp4u(&S.M[b][ty][j], g.mat + c, ok);
+    }
+    const uint32_t ze = z0 + TZ;
+    if (lane == 31) {                                   // high z halo cell
+        const bool ok = rowIn && ze < g.Nz;
+        const size_t c = base + (ok ? ze : 0);
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            cp4(&S.H[b][n][ty + 1][TZ + 1], g.H0 + n * N + c, ok);
+            cp4(&S.E[b][n][ty][TZ + 1], g.V0 + n * N + c, ok);
+        }
+        if (IDX) cp4u(&S.M[b][ty][TZ + 1], g.mat + c, ok);
+    }
+    if (lane == 0) {                                    // low z halo: Hx, Hy at z-1 (self at z = 0)
+        const uint32_t zm = z0 > 0 ? z0 - 1 : z0;
+        const size_t c = base + zm;
+        cp4(&S.H[b][0][ty + 1][0], g.H0 + c, rowIn);
+        cp4(&S.H[b][1][ty + 1][0], g.H0 + N + c, rowIn);
+    }
+    if (ty == 0) {                                      // low y halo: Hx, Hz at y-1 (self at y = 0)
+        const uint32_t ym = y0 > 0 ? y0 - 1 : y0;
+        const size_t bm = (size_t)x * NyNz + (size_t)ym * Nz;
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const uint32_t z = z0 + lane + 32 * k;
+            const bool ok = z < g.Nz;
+            const int j = 1 + 32 * k + lane;
+            cp4(&S.H[b][0][0][j], g.H0 + bm + (ok ? z : 0), ok);
+            cp4(&S.H[b][2][0][j], g.H0 + 2 * N + bm + (ok ? z : 0), ok);
+        }
+        if (lane == 31) {
+            const bool ok = ze < g.Nz;
+            cp4(&S.H[b][0][0][TZ + 1], g.H0 + bm + (ok ? ze : 0), ok);
+            cp4(&S.H[b][2][0][TZ + 1], g.H0 + 2 * N + bm + (ok ? ze : 0), ok);
+        }
+    }
+}
+
+// E update of one cell at column j of row ty from staged data; hpx = H_old(x-1) (y,z comps).
+template <bool IDX, bool PML, int CPT, int TY>
+__device__ __forceinline__ void e_cell(const FusedSmem<CPT, TY>& S, int b, int ty, int j, const FusedGrid& g, size_t c,
+                                       const PmlSet& ps, const PmlSet& pn, uint32_t pmask, uint32_t x, uint32_t y,
+                                       uint32_t z, float hy_xm, float hz_xm, bool write_flux, float en[3]) {
+    const float hx = S.H[b][0][ty + 1][j], hy = S.H[b][1][ty + 1][j], hz = S.H[b][2][ty + 1][j];
+    const float cx = curl4(hz, S.H[b][2][ty][j], hy, S.H[b][1][ty + 1][j - 1]);
+    const float cy = curl4(hx, S.H[b][0][ty + 1][j - 1], hz, hz_xm);
+    const float cz = curl4(hy, hy_xm, hx, S.H[b][0][ty][j]);
+    float kk[6];
+    coeffs_f<IDX>(g, c, IDX ? S.M[b][ty][j] : 0u, 0, kk);
+    const float e0 = S.E[b][0][ty][j], e1 = S.E[b][1][ty][j], e2 = S.E[b][2][ty][j];
+    if (PML && pmask) {
+        en[0] = pml_chain_pp<true>(ps, pn, pmask, x, y, z, 0, e0, true, kk[0], kk[3], cx, write_flux);
+        en[1] = pml_chain_pp<true>(ps, pn, pmask, x, y, z, 1, e1, true, kk[1], kk[4], cy, write_flux);
+        en[2] = pml_chain_pp<true>(ps, pn, pmask, x, y, z, 2, e2, true, kk[2], kk[5], cz, write_flux);
+    } else {
+        en[0] = upd(e0, kk[0], kk[3], cx);
+        en[1] = upd(e1, kk[1], kk[4], cy);
+        en[2] = upd(e2, kk[2], kk[5], cz);
+    }
+}
+
 template <bool IDX, bool PML, int CPT, int TY>
 __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, const PmlSet ps, const PmlSet pn) {
     constexpr int TZ = 32 * CPT;
-    constexpr int W = TZ + 2;                    // column j <-> z = z0 - 1 + j
-    __shared__ float sH[3][TY + 2][W];           // row r <-> y = y0 - 1 + r
-    __shared__ float sE[2][3][TY + 1][W];        // row r <-> y = y0 + r
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FusedSmem<CPT, TY>& S = *reinterpret_cast<FusedSmem<CPT, TY>*>(smem_raw);
     const int lane = threadIdx.x, ty = threadIdx.y;
     const uint32_t z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY;
     const uint32_t y = y0 + ty;
-    const uint32_t zc = z0 + lane;             // cell k: z = zc + 32*k
     const bool rowIn = y < g.Ny;
     const bool own_row = ty < TY;
     const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
     const uint32_t xs = blockIdx.z * g.xchunk;
-    if (xs >= g.Nx) return;                       // whole block idle (uniform)
+    if (xs >= g.Nx) return;                             // whole block idle (uniform)
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
-    const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1; // last plane whose E this block computes
-    const bool extra = (lane == 31) && (z0 + TZ < g.Nz) && rowIn;
+    const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;      // last plane whose E this block computes
     const uint32_t ze = z0 + TZ;
+    const bool extra = (lane == 31) && rowIn && (ze < g.Nz);
+    uint32_t pmask = 0;
+    if (PML) {
+        const uint32_t lo[3] = {xs, y0, z0};
+        const uint32_t hi[3] = {xe, y0 + TY, ze};
+        pmask = region_mask(ps, lo, hi);
+    }
     bool ok[CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) ok[k] = rowIn && (zc + 32 * k < g.Nz);
-    const uint32_t ym = y0 > 0 ? y0 - 1 : y0;      // low y halo row (self at y = 0)
-    const uint32_t zm = z0 > 0 ? z0 - 1 : z0;      // low z halo column (self at z = 0)
+    for (int k = 0; k < CPT; ++k) ok[k] = rowIn && (z0 + lane + 32 * k < g.Nz);
 
-    float hp[CPT][3], hpe[3] = {0.f, 0.f, 0.f};    // H_old(x-1) of my cells (+ halo cell)
+    // H_old(x-1) (y and z components are enough for E; all three for H) of my cells
+    float hp[CPT][3], hpe[2] = {0.f, 0.f};
     uint32_t matp[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) { hp[k][0] = hp[k][1] = hp[k][2] = 0.f; matp[k] = 0; }
     if (xs > 0) {
-        const size_t b = (size_t)(xs - 1) * NyNz + (size_t)y * Nz + zc;
+        const size_t bb = (size_t)(xs - 1) * NyNz + (size_t)y * Nz;
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            float t[CPT];
-            load_cells<CPT>(g.H0 + n * N + b, ok, t);
+        for (int k = 0; k < CPT; ++k)
+            if (ok[k])
 #pragma unroll
-            for (int k = 0; k < CPT; ++k) hp[k][n] = t[k];
-            if (extra) hpe[n] = __ldg(g.H0 + n * N + (size_t)(xs - 1) * NyNz + (size_t)y * Nz + ze);
-        }
+                for (int n = 0; n < 3; ++n) hp[k][n] = __ldg(g.H0 + n * N + bb + z0 + lane + 32 * k);
+        if (extra) { hpe[0] = __ldg(g.H0 + N + bb + ze); hpe[1] = __ldg(g.H0 + 2 * N + bb + ze); }
     }
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) matp[k] = 0;
+    stage_plane<IDX, CPT, TY>(S, xs & 1, g, xs, y0, z0, lane, ty);
+    cp_commit();
 
     for (uint32_t x = xs; x <= xl; ++x) {
-        const size_t b = (size_t)x * NyNz + (size_t)y * Nz + zc;
-        float hc[CPT][3], hce[3] = {0.f, 0.f, 0.f};
-        // ---- 1. stage H_old(x)
-#pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            float t[CPT];
-            load_cells<CPT>(g.H0 + n * N + b, ok, t);
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) { hc[k][n] = t[k]; sH[n][ty + 1][1 + 32 * k + lane] = t[k]; }
-            if (extra) { hce[n] = __ldg(g.H0 + n * N + (size_t)x * NyNz + (size_t)y * Nz + ze); sH[n][ty + 1][TZ + 1] = hce[n]; }
-        }
-        if (ty == 0) {
-            const bool rin = y0 < g.Ny;
-            const size_t bm = (size_t)x * NyNz + (size_t)ym * Nz + zc;
-            bool okm[CPT];
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) okm[k] = rin && (zc + 32 * k < g.Nz);
-#pragma unroll
-            for (int n = 0; n < 3; n += 2) {     // Hx, Hz at y-1
-                float t[CPT];
-                load_cells<CPT>(g.H0 + n * N + bm, okm, t);
-#pragma unroll
-                for (int k = 0; k < CPT; ++k) sH[n][0][1 + 32 * k + lane] = t[k];
-                if (lane == 31 && rin && ze < g.Nz) sH[n][0][TZ + 1] = __ldg(g.H0 + n * N + (size_t)x * NyNz + (size_t)ym * Nz + ze);
-            }
-        }
-        if (lane == 0 && rowIn) {
-            const size_t cz = (size_t)x * NyNz + (size_t)y * Nz + zm;
-            sH[0][ty + 1][0] = __ldg(g.H0 + cz);         // Hx at z-1
-            sH[1][ty + 1][0] = __ldg(g.H0 + N + cz);     // Hy at z-1
-        }
-        // ---- 2. E_old(x), material rows
-        float eo[CPT][3], eoe[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            float t[CPT];
-            load_cells<CPT>(g.V0 + n * N + b, ok, t);
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) eo[k][n] = t[k];
-            if (extra) eoe[n] = __ldg(g.V0 + n * N + (size_t)x * NyNz + (size_t)y * Nz + ze);
-        }
-        uint32_t matc[CPT], mate = 0;
-        if (IDX) {
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) matc[k] = ok[k] ? __ldg(g.mat + b + 32 * k) : 0u;
-            if (extra) mate = __ldg(g.mat + (size_t)x * NyNz + (size_t)y * Nz + ze);
-        } else {
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) matc[k] = 0;
-        }
+        const int b = x & 1;
+        // prefetch plane x+1 while this one is computed
+        if (x < xl) stage_plane<IDX, CPT, TY>(S, b ^ 1, g, x + 1, y0, z0, lane, ty);
+        cp_commit();
+        cp_wait<1>();
         __syncthreads();
-        // ---- 3. E_new(x) on my cells and the halo
-        const bool x0self = (x == 0);
+        const size_t base = (size_t)x * NyNz + (size_t)y * Nz;
+        const bool self = (x == 0);
+        // ---- E_new(x) of my cells (+ the z halo cell on lane 31)
         float en[CPT][3];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const int j = 1 + 32 * k + lane;
-            const uint32_t z = zc + 32 * k;
-            if (!ok[k]) { en[k][0] = en[k][1] = en[k][2] = 0.f; }
-            else {
-                const float hy_xm = x0self ? hc[k][1] : hp[k][1], hz_xm = x0self ? hc[k][2] : hp[k][2];
-                const float cx = curl4(hc[k][2], sH[2][ty][j], hc[k][1], sH[1][ty + 1][j - 1]);
-                const float cy = curl4(hc[k][0], sH[0][ty + 1][j - 1], hc[k][2], hz_xm);
-                const float cz = curl4(hc[k][1], hy_xm, hc[k][0], sH[0][ty][j]);
-                float kk[6];
-                coeffs_f<IDX>(g, b + 32 * k, matc[k], 0, kk);
-                if (PML) {
-                    const bool wr = own_row && x < xe;
-                    en[k][0] = pml_chain_pp<true>(ps, pn, x, y, z, 0, eo[k][0], true, kk[0], kk[3], cx, wr);
-                    en[k][1] = pml_chain_pp<true>(ps, pn, x, y, z, 1, eo[k][1], true, kk[1], kk[4], cy, wr);
-                    en[k][2] = pml_chain_pp<true>(ps, pn, x, y, z, 2, eo[k][2], true, kk[2], kk[5], cz, wr);
-                } else {
-                    en[k][0] = upd(eo[k][0], kk[0], kk[3], cx);
-                    en[k][1] = upd(eo[k][1], kk[1], kk[4], cy);
-                    en[k][2] = upd(eo[k][2], kk[2], kk[5], cz);
-                }
+            const uint32_t z = z0 + lane + 32 * k;
+            if (ok[k]) {
+                const float hy_xm = self ? S.H[b][1][ty + 1][j] : hp[k][1];
+                const float hz_xm = self ? S.H[b][2][ty + 1][j] : hp[k][2];
+                e_cell<IDX, PML, CPT, TY>(S, b, ty, j, g, base + z, ps, pn, pmask, x, y, z, hy_xm, hz_xm,
+                                          own_row && x < xe, en[k]);
+            } else {
+                en[k][0] = en[k][1] = en[k][2] = 0.f;
             }
 #pragma unroll
-            for (int n = 0; n < 3; ++n) sE[x & 1][n][ty][j] = en[k][n];
+            for (int n = 0; n < 3; ++n) S.En[b][n][ty][j] = en[k][n];
         }
         if (lane == 31) {
             float ee[3] = {0.f, 0.f, 0.f};
             if (extra) {
-                const int j = TZ + 1;
-                const float hy_xm = x0self ? hce[1] : hpe[1], hz_xm = x0self ? hce[2] : hpe[2];
-                const float cx = curl4(hce[2], sH[2][ty][j], hce[1], sH[1][ty + 1][j - 1]);
-                const float cy = curl4(hce[0], sH[0][ty + 1][j - 1], hce[2], hz_xm);
-                const float cz = curl4(hce[1], hy_xm, hce[0], sH[0][ty][j]);
-                float kk[6];
-                const size_t ce = (size_t)x * NyNz + (size_t)y * Nz + ze;
-                coeffs_f<IDX>(g, ce, mate, 0, kk);
-                if (PML) {
-                    ee[0] = pml_chain_pp<true>(ps, pn, x, y, ze, 0, eoe[0], true, kk[0], kk[3], cx, false);
-                    ee[1] = pml_chain_pp<true>(ps, pn, x, y, ze, 1, eoe[1], true, kk[1], kk[4], cy, false);
-                    ee[2] = pml_chain_pp<true>(ps, pn, x, y, ze, 2, eoe[2], true, kk[2], kk[5], cz, false);
-                } else {
-                    ee[0] = upd(eoe[0], kk[0], kk[3], cx);
-                    ee[1] = upd(eoe[1], kk[1], kk[4], cy);
-                    ee[2] = upd(eoe[2], kk[2], kk[5], cz);
-                }
+                const float hy_xm = self ? S.H[b][1][ty + 1][TZ + 1] : hpe[0];
+                const float hz_xm = self ? S.H[b][2][ty + 1][TZ + 1] : hpe[1];
+                e_cell<IDX, PML, CPT, TY>(S, b, ty, TZ + 1, g, base + ze, ps, pn, pmask, x, y, ze, hy_xm, hz_xm, false, ee);
+                hpe[0] = S.H[b][1][ty + 1][TZ + 1];
+                hpe[1] = S.H[b][2][ty + 1][TZ + 1];
             }
 #pragma unroll
-            for (int n = 0; n < 3; ++n) sE[x & 1][n][ty][TZ + 1] = ee[n];
+            for (int n = 0; n < 3; ++n) S.En[b][n][ty][TZ + 1] = ee[n];
         }
         if (own_row && x < xe) {
 #pragma unroll
-            for (int n = 0; n < 3; ++n) {
-                float t[CPT];
+            for (int k = 0; k < CPT; ++k)
+                if (ok[k])
 #pragma unroll
-                for (int k = 0; k < CPT; ++k) t[k] = en[k][n];
-                store_cells<CPT>(g.V1 + n * N + b, ok, t);
-            }
+                    for (int n = 0; n < 3; ++n) g.V1[n * N + base + z0 + lane + 32 * k] = en[k][n];
+        }
+        // H_old(x) and the material rows of my cells, needed for H(x) in the next iteration
+        float hc[CPT][3];
+        uint32_t matc[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int j = 1 + 32 * k + lane;
+#pragma unroll
+            for (int n = 0; n < 3; ++n) hc[k][n] = S.H[b][n][ty + 1][j];
+            matc[k] = IDX ? S.M[b][ty][j] : 0u;
         }
         __syncthreads();
-        // ---- 4. H_new(x-1) on my cells
+        // ---- H_new(x-1) of my cells
         if (own_row && x > xs) {
-            const int pe = (x - 1) & 1;
-            const size_t bm1 = b - NyNz;
-            float hn[CPT][3];
-            bool wr[CPT];
+            const int pe = b ^ 1;
+            const size_t bm1 = base - NyNz;
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
+                if (!ok[k]) continue;
                 const int j = 1 + 32 * k + lane;
-                const uint32_t z = zc + 32 * k;
-                wr[k] = ok[k];
-                if (ok[k] && g.defer) {
-                    const size_t cm = bm1 + 32 * k;
-                    if ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) wr[k] = false;
-                }
-                hn[k][0] = hn[k][1] = hn[k][2] = 0.f;
-                if (!wr[k]) continue;
+                const uint32_t z = z0 + lane + 32 * k;
+                const size_t cm = bm1 + z;
+                if (g.defer && ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u)) continue;
                 const bool core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
                 float cx = 0.f, cy = 0.f, cz = 0.f;
-                if (core) {
-                    const float ex = sE[pe][0][ty][j], ey = sE[pe][1][ty][j], ez = sE[pe][2][ty][j];
-                    cx = curl4(ez, sE[pe][2][ty + 1][j], ey, sE[pe][1][ty][j + 1]);
-                    cy = curl4(ex, sE[pe][0][ty][j + 1], ez, en[k][2]);
-                    cz = curl4(ey, en[k][1], ex, sE[pe][0][ty + 1][j]);
-                }
                 float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                if (core) coeffs_f<IDX>(g, bm1 + 32 * k, matp[k], 6, kk);
-                if (PML) {
-                    hn[k][0] = pml_chain_pp<false>(ps, pn, x - 1, y, z, 0, hp[k][0], core, kk[0], kk[3], cx, true);
-                    hn[k][1] = pml_chain_pp<false>(ps, pn, x - 1, y, z, 1, hp[k][1], core, kk[1], kk[4], cy, true);
-                    hn[k][2] = pml_chain_pp<false>(ps, pn, x - 1, y, z, 2, hp[k][2], core, kk[2], kk[5], cz, true);
-                } else if (core) {
-                    hn[k][0] = upd(hp[k][0], kk[0], kk[3], cx);
-                    hn[k][1] = upd(hp[k][1], kk[1], kk[4], cy);
-                    hn[k][2] = upd(hp[k][2], kk[2], kk[5], cz);
-                } else {
-                    hn[k][0] = hp[k][0]; hn[k][1] = hp[k][1]; hn[k][2] = hp[k][2];
+                if (core) {
+                    const float ex = S.En[pe][0][ty][j], ey = S.En[pe][1][ty][j], ez = S.En[pe][2][ty][j];
+                    cx = curl4(ez, S.En[pe][2][ty + 1][j], ey, S.En[pe][1][ty][j + 1]);
+                    cy = curl4(ex, S.En[pe][0][ty][j + 1], ez, en[k][2]);
+                    cz = curl4(ey, en[k][1], ex, S.En[pe][0][ty + 1][j]);
+                    coeffs_f<IDX>(g, cm, matp[k], 6, kk);
                 }
-            }
+                float hn[3];
+                if (PML && pmask) {
 #pragma unroll
-            for (int n = 0; n < 3; ++n) {
-                float t[CPT];
+                    for (int n = 0; n < 3; ++n)
+                        hn[n] = pml_chain_pp<false>(ps, pn, pmask, x - 1, y, z, n, hp[k][n], core, kk[n], kk[3 + n],
+                                                    n == 0 ? cx : (n == 1 ? cy : cz), true);
+                } else if (core) {
+                    hn[0] = upd(hp[k][0], kk[0], kk[3], cx);
+                    hn[1] = upd(hp[k][1], kk[1], kk[4], cy);
+                    hn[2] = upd(hp[k][2], kk[2], kk[5], cz);
+                } else {
+                    hn[0] = hp[k][0]; hn[1] = hp[k][1]; hn[2] = hp[k][2];
+                }
 #pragma unroll
-                for (int k = 0; k < CPT; ++k) t[k] = hn[k][n];
-                store_cells<CPT>(g.H1 + n * N + bm1, wr, t);
+                for (int n = 0; n < 3; ++n) g.H1[n * N + cm] = hn[n];
             }
         }
-        // ---- rotate
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             hp[k][0] = hc[k][0]; hp[k][1] = hc[k][1]; hp[k][2] = hc[k][2];
             matp[k] = matc[k];
         }
-        hpe[0] = hce[0]; hpe[1] = hce[1]; hpe[2] = hce[2];
     }
+    cp_wait<0>();
     // ---- H of the last plane x = Nx-1: no core update (loop bounds), UPML / pass-through only
     if (xe == g.Nx && own_row) {
-        const size_t bl = (size_t)(g.Nx - 1) * NyNz + (size_t)y * Nz + zc;
-        float hn[CPT][3];
-        bool wr[CPT];
+        const size_t bl = (size_t)(g.Nx - 1) * NyNz + (size_t)y * Nz;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            wr[k] = ok[k];
-            if (ok[k] && g.defer) {
-                const size_t cm = bl + 32 * k;
-                if ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) wr[k] = false;
-            }
+            if (!ok[k]) continue;
+            const uint32_t z = z0 + lane + 32 * k;
+            const size_t cm = bl + z;
+            if (g.defer && ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u)) continue;
 #pragma unroll
             for (int n = 0; n < 3; ++n)
-                hn[k][n] = (PML && wr[k]) ? pml_chain_pp<false>(ps, pn, g.Nx - 1, y, zc + 32 * k, n, hp[k][n], false, 0.f, 0.f, 0.f, true)
-                                          : hp[k][n];
-        }
-#pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            float t[CPT];
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) t[k] = hn[k][n];
-            store_cells<CPT>(g.H1 + n * N + bl, wr, t);
+                g.H1[n * N + cm] = (PML && pmask) ? pml_chain_pp<false>(ps, pn, pmask, g.Nx - 1, y, z, n, hp[k][n], false, 0.f, 0.f, 0.f, true)
+                                                  : hp[k][n];
         }
     }
 }
@@ -357,7 +388,7 @@ __global__ void k_deferred_h(const FusedGrid g, const PmlSet ps, const PmlSet pn
     for (int q = 0; q < 3; ++q) {
         const float ho = g.H0[q * N + c];
         float hn;
-        if (PML) hn = pml_chain_pp<false>(ps, pn, x, y, z, q, ho, core, kk[q], kk[3 + q], q == 0 ? cx : (q == 1 ? cy : cz), true);
+        if (PML) hn = pml_chain_pp<false>(ps, pn, ps.count >= 32 ? ~0u : ((1u << ps.count) - 1u), x, y, z, q, ho, core, kk[q], kk[3 + q], q == 0 ? cx : (q == 1 ? cy : cz), true);
         else hn = core ? upd(ho, kk[q], kk[3 + q], q == 0 ? cx : (q == 1 ? cy : cz)) : ho;
         g.H1[q * N + c] = hn;
     }

@@ -55,6 +55,21 @@ __device__ __forceinline__ float curl4(float a, float b, float c, float d) {
 __device__ __forceinline__ bool in_region(const PmlRegion& r, uint32_t x, uint32_t y, uint32_t z) {
     return (x - r.s[0]) < r.n[0] && (y - r.s[1]) < r.n[1] && (z - r.s[2]) < r.n[2];
 }
+
+// Regions intersecting the box [lo, hi] (inclusive), as a bit mask.  Blocks
+// compute this once so cells of tiles that touch no UPML region skip the
+// per-cell membership tests entirely.
+__device__ __forceinline__ uint32_t region_mask(const PmlSet& ps, const uint32_t lo[3], const uint32_t hi[3]) {
+    uint32_t m = 0;
+    for (int r = 0; r < ps.count; ++r) {
+        bool hit = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            hit = hit && (hi[d] >= ps.r[r].s[d]) && (lo[d] < ps.r[r].s[d] + ps.r[r].n[d]);
+        if (hit) m |= 1u << r;
+    }
+    return m;
+}
 __device__ __forceinline__ size_t region_p(const PmlRegion& r, uint32_t n, uint32_t x, uint32_t y, uint32_t z) {
     size_t nyz = (size_t)r.n[1] * r.n[2];
     return (size_t)n * r.n[0] * nyz + (size_t)(x - r.s[0]) * nyz + (size_t)(y - r.s[1]) * r.n[2] + (z - r.s[2]);
@@ -64,11 +79,13 @@ __device__ __forceinline__ size_t region_p(const PmlRegion& r, uint32_t n, uint3
 // (src/webgpu-fdtd.mjs:239-358 around :1138/:1162).  `core` false: the core
 // update skips this cell (current loop bounds) but UPML still swaps.
 template <bool VOLT>
-__device__ __forceinline__ float pml_chain(const PmlSet& ps, uint32_t x, uint32_t y, uint32_t z, uint32_t n,
+__device__ __forceinline__ float pml_chain(const PmlSet& ps, uint32_t mask, uint32_t x, uint32_t y, uint32_t z, uint32_t n,
                                            float vold, bool core, float cv, float ci, float curl) {
     int cnt = 0, only = -1;
-    for (int r = 0; r < ps.count; ++r)
+    for (uint32_t m = mask; m; m &= m - 1) {
+        const int r = __ffs(m) - 1;
         if (in_region(ps.r[r], x, y, z)) { ++cnt; only = r; }
+    }
     if (cnt == 0) return core ? upd(vold, cv, ci, curl) : vold;
     if (cnt == 1) {
         const PmlRegion& R = ps.r[only];
@@ -138,6 +155,12 @@ __global__ void __launch_bounds__(256) k_volt(const Grid g, const PmlSet ps) {
     const size_t sy = y > 0 ? g.Nz : 0, sz = z > 0 ? 1 : 0;
     const float* __restrict__ H = g.curr;
     float* __restrict__ V = g.volt;
+    uint32_t pmask = 0;
+    if (PML) {
+        const uint32_t lo[3] = {x0, blockIdx.y * CORE_BY, blockIdx.x * CORE_BZ};
+        const uint32_t hi[3] = {x1 - 1, lo[1] + CORE_BY - 1, lo[2] + CORE_BZ - 1};
+        pmask = region_mask(ps, lo, hi);
+    }
     size_t c = (size_t)x0 * NyNz + (size_t)y * g.Nz + z;
     float hy_p, hz_p;
     if (x0 > 0) { hy_p = __ldg(H + N + c - NyNz); hz_p = __ldg(H + 2 * N + c - NyNz); }
@@ -152,10 +175,10 @@ __global__ void __launch_bounds__(256) k_volt(const Grid g, const PmlSet ps) {
         float k[6];
         coeffs<IDX>(g, c, 0, k);
         const float e0 = V[c], e1 = V[N + c], e2 = V[2 * N + c];
-        if (PML) {
-            V[c] = pml_chain<true>(ps, x, y, z, 0, e0, true, k[0], k[3], cx);
-            V[N + c] = pml_chain<true>(ps, x, y, z, 1, e1, true, k[1], k[4], cy);
-            V[2 * N + c] = pml_chain<true>(ps, x, y, z, 2, e2, true, k[2], k[5], cz);
+        if (PML && pmask) {
+            V[c] = pml_chain<true>(ps, pmask, x, y, z, 0, e0, true, k[0], k[3], cx);
+            V[N + c] = pml_chain<true>(ps, pmask, x, y, z, 1, e1, true, k[1], k[4], cy);
+            V[2 * N + c] = pml_chain<true>(ps, pmask, x, y, z, 2, e2, true, k[2], k[5], cz);
         } else {
             V[c] = upd(e0, k[0], k[3], cx);
             V[N + c] = upd(e1, k[1], k[4], cy);
@@ -176,7 +199,13 @@ __global__ void __launch_bounds__(256) k_curr(const Grid g, const PmlSet ps) {
     const uint32_t x1 = min(x0 + CORE_TX, g.Nx);
     const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
     const bool yz_core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
-    if (!PML && !yz_core) return;
+    uint32_t pmask = 0;
+    if (PML) {
+        const uint32_t lo[3] = {x0, blockIdx.y * CORE_BY, blockIdx.x * CORE_BZ};
+        const uint32_t hi[3] = {x1 - 1, lo[1] + CORE_BY - 1, lo[2] + CORE_BZ - 1};
+        pmask = region_mask(ps, lo, hi);
+    }
+    if (!pmask && !yz_core) return;
     const float* __restrict__ V = g.volt;
     float* __restrict__ H = g.curr;
     size_t c = (size_t)x0 * NyNz + (size_t)y * Nz + z;
@@ -195,13 +224,13 @@ __global__ void __launch_bounds__(256) k_curr(const Grid g, const PmlSet ps) {
             cz = curl4(ey_c, ey_xp, ex, ex_yp);
             ey_c = ey_xp; ez_c = ez_xp;
         }
-        if (PML) {
+        if (PML && pmask) {
             float k[6] = {0, 0, 0, 0, 0, 0};
             if (core) coeffs<IDX>(g, c, 6, k);
             const float h0 = H[c], h1 = H[N + c], h2 = H[2 * N + c];
-            const float r0 = pml_chain<false>(ps, x, y, z, 0, h0, core, k[0], k[3], cx);
-            const float r1 = pml_chain<false>(ps, x, y, z, 1, h1, core, k[1], k[4], cy);
-            const float r2 = pml_chain<false>(ps, x, y, z, 2, h2, core, k[2], k[5], cz);
+            const float r0 = pml_chain<false>(ps, pmask, x, y, z, 0, h0, core, k[0], k[3], cx);
+            const float r1 = pml_chain<false>(ps, pmask, x, y, z, 1, h1, core, k[1], k[4], cy);
+            const float r2 = pml_chain<false>(ps, pmask, x, y, z, 2, h2, core, k[2], k[5], cz);
             if (core || r0 != h0 || r1 != h1 || r2 != h2) { H[c] = r0; H[N + c] = r1; H[2 * N + c] = r2; }
             // (bitwise-equal rewrites of untouched cells are skipped; NaN != NaN rewrites are harmless)
         } else if (core) {

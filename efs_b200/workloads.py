@@ -244,6 +244,30 @@ def probe_series(engine, job, slices):
     return opgen.probe_integrals(g, job["probes"], slices)
 
 
+def far_field_summary(engine, job, freq_index=0, dtheta=3.0, dphi=5.0, far_field_fn=None):
+    """The orchestrator's NF2FF post-processing (sim-engine.mjs:725-806):
+    far field on a theta x phi grid (3 and 5 degrees as the Node runner),
+    radiated power through the surface, Dmax = 4 pi P_max r^2 / P_rad.
+    far_field_fn(accE, accH, meta, theta, phi, freq) replaces the engine's
+    far-field kernel (tests pass the f64 oracle)."""
+    theta = np.deg2rad(np.arange(0.0, 180.0 + 1e-9, dtheta)).astype(np.float32)
+    phi = np.deg2rad(np.arange(0.0, 360.0 + 1e-9, dphi)).astype(np.float32)
+    acc = engine.readNF2FFAccumulation(True)
+    meta = job["nf2ff_meta"]
+    freq = job["nf2ff_freqs"][freq_index]
+    if far_field_fn is None:
+        out = engine.computeNF2FFfarField(dict(pointMeta=meta, theta=theta, phi=phi, center=[0, 0, 0], frequency=freq,
+                                               radius=1.0, numPoints=job["nf2ff"]["numPoints"],
+                                               freqIndex=freq_index)).reshape(-1, 5).astype(np.float64)
+    else:
+        out = far_field_fn(acc["accumE"][freq_index], acc["accumH"][freq_index], meta, theta, phi, freq)
+    p_max = float(out[:, 0].max())
+    prad = opgen.rad_power(acc["accumE"][freq_index], acc["accumH"][freq_index], meta)
+    dmax = p_max * 4 * math.pi / prad if prad > 0 else 0.0
+    return {"freqHz": freq, "P_max": p_max, "P_rad": prad, "Dmax": dmax,
+            "DmaxdBi": 10 * math.log10(max(dmax, 1e-15)), "pattern": out}
+
+
 def run_probe_job(engine, job):
     """Run a probe-only job; returns the first probe's series (with t = 0 if the
     job's reference data starts there)."""

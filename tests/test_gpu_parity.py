@@ -23,15 +23,16 @@ pytestmark = pytest.mark.gpu
 # inside the test grids) and the separate E/H sweeps.
 CORES = {
     "fused": {},
-    "fused_cpt4_x3": {"EFS_CPT": "4", "EFS_XCHUNK": "3"},
-    "fused_cpt1_x5": {"EFS_CPT": "1", "EFS_XCHUNK": "5"},
+    "fused_cpt2_x3": {"EFS_CPT": "2", "EFS_XCHUNK": "3"},
+    "fused_ty16_x5": {"EFS_TY": "16", "EFS_XCHUNK": "5"},
+    "fused_cpt2_ty16": {"EFS_CPT": "2", "EFS_TY": "16"},
     "split": {"EFS_CORE": "split"},
 }
 
 
 @pytest.fixture(autouse=True, params=list(CORES))
 def core_path(request, monkeypatch):
-    for k in ("EFS_CORE", "EFS_CPT", "EFS_XCHUNK"):
+    for k in ("EFS_CORE", "EFS_CPT", "EFS_XCHUNK", "EFS_TY"):
         monkeypatch.delenv(k, raising=False)
     for k, v in CORES[request.param].items():
         monkeypatch.setenv(k, v)
