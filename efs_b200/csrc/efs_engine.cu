@@ -90,7 +90,9 @@ struct efs_engine {
     int cur = 0;                // parity holding the current fields
     uint32_t xchunk = 64;       // x-planes per block of the fused kernel
     int cpt = 1;                // z cells per thread of the fused kernel (1 or 2)
-    int ty_rows = 8;            // y rows per tile of the fused kernel (8 or 16)
+    int ty_rows = 8;            // y rows per tile of the shared-memory fused kernel (8 or 16)
+    int fused_kind = 0;         // 0: register-blocked fused kernel, 1: shared-memory tiled fused kernel
+    int ry = 4;                 // y rows per thread of the register-blocked kernel (2, 4, 8)
     DevBuf defer_bits, defer_cells;
     uint32_t defer_n = 0;
     std::vector<uint32_t> h_exc_targets, h_tfsf_v_targets, h_mur_apply, h_rlc_series;
@@ -447,7 +449,22 @@ struct efs_engine {
         if (indexed) { if (hp) launch_fused_k<true, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<true, false, CPT, TY>(g, b, fg, ps, pn); }
         else { if (hp) launch_fused_k<false, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<false, false, CPT, TY>(g, b, fg, ps, pn); }
     }
+    template <int RY>
+    void launch_fused_reg(int p) {
+        const FusedGrid fg = fused_grid(p);
+        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
+        dim3 b(32, 4), g(blocks(Nz, RZ), blocks(Ny, 4 * RY), blocks(Nx, xchunk));
+        const bool hp = !pml.empty();
+        if (indexed) { if (hp) k_fused_reg<true, true, RY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<true, false, RY><<<g, b, 0, stream>>>(fg, ps, pn); }
+        else { if (hp) k_fused_reg<false, true, RY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<false, false, RY><<<g, b, 0, stream>>>(fg, ps, pn); }
+    }
     void launch_fused(int p) {
+        if (fused_kind == 0) {
+            if (ry >= 8) launch_fused_reg<8>(p);
+            else if (ry >= 4) launch_fused_reg<4>(p);
+            else launch_fused_reg<2>(p);
+            return;
+        }
         if (cpt >= 2) { if (ty_rows >= 16) launch_fused_t<2, 16>(p); else launch_fused_t<2, 8>(p); }
         else { if (ty_rows >= 16) launch_fused_t<1, 16>(p); else launch_fused_t<1, 8>(p); }
     }
@@ -581,6 +598,8 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     if (const char* s = getenv("EFS_XCHUNK")) e->xchunk = std::max(1, atoi(s));
     if (const char* s = getenv("EFS_CPT")) e->cpt = std::max(1, atoi(s));
     if (const char* s = getenv("EFS_TY")) e->ty_rows = std::max(8, atoi(s));
+    if (const char* s = getenv("EFS_FUSED")) e->fused_kind = std::string(s) == "smem" ? 1 : 0;
+    if (const char* s = getenv("EFS_RY")) e->ry = std::max(2, atoi(s));
     e->cur = 0;
     e->alloc(e->volt, 3 * N * sizeof(float));
     e->alloc(e->curr, 3 * N * sizeof(float));

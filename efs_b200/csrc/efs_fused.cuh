@@ -365,6 +365,186 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
     }
 }
 
+// ---------------------------------------------------------------------------
+// Register-blocked variant (default): no shared memory, no block barriers.
+// A warp covers 32 consecutive z (lane l <-> z = z0 + l - 1, z0 = 30*tile):
+// lanes 1..30 own their cells, lane 0 only supplies H(z0-1) and lane 31
+// computes the E halo at z0+30; z neighbours travel by warp shuffles.  Each
+// thread owns RY consecutive y rows, computes E on RY+1 rows (the extra row
+// is the y halo) and keeps the previous plane's H_old and E_new in registers
+// while it streams x.  Every warp is independent, so the SM keeps many
+// planes' loads in flight.
+// ---------------------------------------------------------------------------
+constexpr int RZ = 30;          // owned z per warp
+
+template <bool IDX, bool PML, int RY>
+__global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlSet ps, const PmlSet pn) {
+    const int lane = threadIdx.x;
+    const uint32_t z0 = blockIdx.x * RZ;
+    const int64_t zl = (int64_t)z0 + lane - 1;                  // this lane's z
+    const uint32_t zload = zl < 0 ? 0u : (uint32_t)zl;           // z = -1 loads z = 0 (self reference)
+    const bool zin = zl < (int64_t)g.Nz;
+    const bool own_z = lane >= 1 && lane <= RZ && zin;
+    const uint32_t y0 = (blockIdx.y * blockDim.y + threadIdx.y) * RY;
+    if (y0 >= g.Ny) return;                                      // whole warp idle (uniform per warp)
+    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
+    const uint32_t xs = blockIdx.z * g.xchunk;
+    if (xs >= g.Nx) return;
+    const uint32_t xe = min(xs + g.xchunk, g.Nx);
+    const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;
+    const uint32_t z = (uint32_t)(zl < 0 ? 0 : zl);
+    uint32_t pmask = 0;
+    if (PML) {
+        const uint32_t lo[3] = {xs, y0 > 0 ? y0 - 1 : 0, z0 > 0 ? z0 - 1 : 0};
+        const uint32_t hi[3] = {xe, y0 + RY, z0 + RZ};
+        pmask = region_mask(ps, lo, hi);
+    }
+    bool rin[RY + 1];
+#pragma unroll
+    for (int r = 0; r <= RY; ++r) rin[r] = (y0 + r < g.Ny) && zin;
+    const uint32_t ym = y0 > 0 ? y0 - 1 : y0;                    // y = -1 reads y = 0 (self reference)
+
+    float hp[RY + 1][3];     // H_old(x-1) rows y0..y0+RY
+    float ep[RY + 1][3];     // E_new(x-1) rows y0..y0+RY
+    uint32_t mp[RY];         // material rows of plane x-1 (owned rows)
+#pragma unroll
+    for (int r = 0; r <= RY; ++r) { hp[r][0] = hp[r][1] = hp[r][2] = 0.f; ep[r][0] = ep[r][1] = ep[r][2] = 0.f; }
+#pragma unroll
+    for (int r = 0; r < RY; ++r) mp[r] = 0;
+    if (xs > 0) {
+        const size_t b = (size_t)(xs - 1) * NyNz + zload;
+#pragma unroll
+        for (int r = 0; r <= RY; ++r)
+            if (rin[r]) {
+                const size_t c = b + (size_t)(y0 + r) * Nz;
+                hp[r][1] = __ldg(g.H0 + N + c);
+                hp[r][2] = __ldg(g.H0 + 2 * N + c);
+            }
+    }
+    for (uint32_t x = xs; x <= xl; ++x) {
+        const size_t bx = (size_t)x * NyNz + zload;
+        // ---- loads of plane x: H rows y0-1..y0+RY, E_old and material rows y0..y0+RY
+        float h[RY + 2][3], eo[RY + 1][3];
+        uint32_t m[RY + 1];
+        {
+            const size_t c = bx + (size_t)ym * Nz;
+            h[0][0] = zin ? __ldg(g.H0 + c) : 0.f;
+            h[0][1] = 0.f;
+            h[0][2] = zin ? __ldg(g.H0 + 2 * N + c) : 0.f;
+        }
+#pragma unroll
+        for (int r = 0; r <= RY; ++r) {
+            const size_t c = bx + (size_t)(y0 + r) * Nz;
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                h[r + 1][n] = rin[r] ? __ldg(g.H0 + n * N + c) : 0.f;
+                eo[r][n] = rin[r] ? __ldg(g.V0 + n * N + c) : 0.f;
+            }
+            m[r] = (IDX && rin[r]) ? __ldg(g.mat + c) : 0u;
+        }
+        uint32_t dbits[RY];
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            dbits[r] = 0;
+            if (g.defer && x > xs && own_z && rin[r]) {
+                const size_t cm = (size_t)(x - 1) * NyNz + (size_t)(y0 + r) * Nz + z;
+                dbits[r] = (__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u;
+            }
+        }
+        const bool self = (x == 0);
+        // ---- E_new(x) on rows y0..y0+RY (row RY is the y halo), lanes 1..31
+        float en[RY + 1][3];
+#pragma unroll
+        for (int r = 0; r <= RY; ++r) {
+            const float hx = h[r + 1][0], hy = h[r + 1][1], hz = h[r + 1][2];
+            const float hy_zm = __shfl_up_sync(0xffffffffu, hy, 1);
+            const float hx_zm = __shfl_up_sync(0xffffffffu, hx, 1);
+            const float hy_xm = self ? hy : hp[r][1], hz_xm = self ? hz : hp[r][2];
+            const float cx = curl4(hz, h[r][2], hy, hy_zm);
+            const float cy = curl4(hx, hx_zm, hz, hz_xm);
+            const float cz = curl4(hy, hy_xm, hx, h[r][0]);
+            en[r][0] = en[r][1] = en[r][2] = 0.f;
+            if (lane >= 1 && rin[r]) {
+                const size_t c = bx + (size_t)(y0 + r) * Nz;
+                float kk[6];
+                coeffs_f<IDX>(g, c, m[r], 0, kk);
+                if (PML && pmask) {
+                    const bool wr = own_z && r < RY && x < xe;
+                    en[r][0] = pml_chain_pp<true>(ps, pn, pmask, x, y0 + r, z, 0, eo[r][0], true, kk[0], kk[3], cx, wr);
+                    en[r][1] = pml_chain_pp<true>(ps, pn, pmask, x, y0 + r, z, 1, eo[r][1], true, kk[1], kk[4], cy, wr);
+                    en[r][2] = pml_chain_pp<true>(ps, pn, pmask, x, y0 + r, z, 2, eo[r][2], true, kk[2], kk[5], cz, wr);
+                } else {
+                    en[r][0] = upd(eo[r][0], kk[0], kk[3], cx);
+                    en[r][1] = upd(eo[r][1], kk[1], kk[4], cy);
+                    en[r][2] = upd(eo[r][2], kk[2], kk[5], cz);
+                }
+                if (own_z && r < RY && x < xe) {
+                    g.V1[c] = en[r][0];
+                    g.V1[N + c] = en[r][1];
+                    g.V1[2 * N + c] = en[r][2];
+                }
+            }
+        }
+        // ---- H_new(x-1) on owned rows and lanes
+        if (x > xs) {
+#pragma unroll
+            for (int r = 0; r < RY; ++r) {
+                const float ey_zp = __shfl_down_sync(0xffffffffu, ep[r][1], 1);
+                const float ex_zp = __shfl_down_sync(0xffffffffu, ep[r][0], 1);
+                if (!own_z || !rin[r] || dbits[r]) continue;
+                const uint32_t y = y0 + r;
+                const size_t cm = (size_t)(x - 1) * NyNz + (size_t)y * Nz + z;
+                const bool core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
+                float cx = 0.f, cy = 0.f, cz = 0.f;
+                float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (core) {
+                    cx = curl4(ep[r][2], ep[r + 1][2], ep[r][1], ey_zp);
+                    cy = curl4(ep[r][0], ex_zp, ep[r][2], en[r][2]);
+                    cz = curl4(ep[r][1], en[r][1], ep[r][0], ep[r + 1][0]);
+                    coeffs_f<IDX>(g, cm, mp[r], 6, kk);
+                }
+                float hn[3];
+                if (PML && pmask) {
+#pragma unroll
+                    for (int n = 0; n < 3; ++n)
+                        hn[n] = pml_chain_pp<false>(ps, pn, pmask, x - 1, y, z, n, hp[r][n], core, kk[n], kk[3 + n],
+                                                    n == 0 ? cx : (n == 1 ? cy : cz), true);
+                } else if (core) {
+                    hn[0] = upd(hp[r][0], kk[0], kk[3], cx);
+                    hn[1] = upd(hp[r][1], kk[1], kk[4], cy);
+                    hn[2] = upd(hp[r][2], kk[2], kk[5], cz);
+                } else {
+                    hn[0] = hp[r][0]; hn[1] = hp[r][1]; hn[2] = hp[r][2];
+                }
+                g.H1[cm] = hn[0];
+                g.H1[N + cm] = hn[1];
+                g.H1[2 * N + cm] = hn[2];
+            }
+        }
+        // ---- rotate
+#pragma unroll
+        for (int r = 0; r <= RY; ++r) {
+            hp[r][0] = h[r + 1][0]; hp[r][1] = h[r + 1][1]; hp[r][2] = h[r + 1][2];
+            ep[r][0] = en[r][0]; ep[r][1] = en[r][1]; ep[r][2] = en[r][2];
+        }
+#pragma unroll
+        for (int r = 0; r < RY; ++r) mp[r] = m[r];
+    }
+    // ---- H of the last plane x = Nx-1: no core update, UPML / pass-through only
+    if (xe == g.Nx && own_z) {
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            if (!rin[r]) continue;
+            const size_t cm = (size_t)(g.Nx - 1) * NyNz + (size_t)(y0 + r) * Nz + z;
+            if (g.defer && ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u)) continue;
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+                g.H1[n * N + cm] = (PML && pmask) ? pml_chain_pp<false>(ps, pn, pmask, g.Nx - 1, y0 + r, z, n, hp[r][n], false, 0.f, 0.f, 0.f, true)
+                                                  : hp[r][n];
+        }
+    }
+}
+
 // H update of the deferred cells, after the E-side sparse operations:
 // reads the final E_new, H_old, writes H_new (with UPML), one thread per cell.
 template <bool IDX, bool PML>

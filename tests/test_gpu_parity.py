@@ -23,16 +23,17 @@ pytestmark = pytest.mark.gpu
 # inside the test grids) and the separate E/H sweeps.
 CORES = {
     "fused": {},
-    "fused_cpt2_x3": {"EFS_CPT": "2", "EFS_XCHUNK": "3"},
-    "fused_ty16_x5": {"EFS_TY": "16", "EFS_XCHUNK": "5"},
-    "fused_cpt2_ty16": {"EFS_CPT": "2", "EFS_TY": "16"},
+    "fused_ry2_x3": {"EFS_RY": "2", "EFS_XCHUNK": "3"},
+    "fused_ry8_x5": {"EFS_RY": "8", "EFS_XCHUNK": "5"},
+    "fused_smem_cpt2_x3": {"EFS_FUSED": "smem", "EFS_CPT": "2", "EFS_XCHUNK": "3"},
+    "fused_smem_ty16": {"EFS_FUSED": "smem", "EFS_TY": "16"},
     "split": {"EFS_CORE": "split"},
 }
 
 
 @pytest.fixture(autouse=True, params=list(CORES))
 def core_path(request, monkeypatch):
-    for k in ("EFS_CORE", "EFS_CPT", "EFS_XCHUNK", "EFS_TY"):
+    for k in ("EFS_CORE", "EFS_CPT", "EFS_XCHUNK", "EFS_TY", "EFS_FUSED", "EFS_RY"):
         monkeypatch.delenv(k, raising=False)
     for k, v in CORES[request.param].items():
         monkeypatch.setenv(k, v)
