@@ -72,6 +72,40 @@ __device__ __forceinline__ float pml_chain_pp(const PmlSet& ps, const PmlSet& pn
     return v;
 }
 
+// UPML chain for a cell whose containing regions are exactly the set bits of
+// `cell_mask` (already intersected per axis by the caller).  The single-region
+// case (slab interiors) runs in registers; overlaps (corners) use the general chain.
+template <bool VOLT>
+__device__ __forceinline__ float pml_cell(const PmlSet& ps, const PmlSet& pn, uint32_t cell_mask, uint32_t x, uint32_t y,
+                                          uint32_t z, uint32_t n, float vold, bool core, float cv, float ci, float curl,
+                                          bool write) {
+    if (cell_mask == 0) return core ? upd(vold, cv, ci, curl) : vold;
+    if ((cell_mask & (cell_mask - 1)) == 0) {
+        const int r = __ffs(cell_mask) - 1;
+        const PmlRegion& R = ps.r[r];
+        const size_t p = region_p(R, n, x, y, z);
+        const float a = VOLT ? R.vv[p] : R.ii[p];
+        const float b = VOLT ? R.vvfo[p] : R.iifo[p];
+        const float fn = VOLT ? R.vvfn[p] : R.iifn[p];
+        const float fo = VOLT ? R.vflux[p] : R.cflux[p];
+        const float fh = __fsub_rn(__fmul_rn(a, vold), __fmul_rn(b, fo));
+        const float v = core ? upd(fo, cv, ci, curl) : fo;
+        if (write) (VOLT ? pn.r[r].vflux : pn.r[r].cflux)[p] = v;
+        return __fadd_rn(fh, __fmul_rn(fn, v));
+    }
+    return pml_chain_pp<VOLT>(ps, pn, cell_mask, x, y, z, n, vold, core, cv, ci, curl, write);
+}
+
+// Regions (bit mask) whose extent along `axis` contains coordinate c.
+__device__ __forceinline__ uint32_t axis_mask(const PmlSet& ps, uint32_t cand, int axis, uint32_t c) {
+    uint32_t m = 0;
+    for (uint32_t b = cand; b; b &= b - 1) {
+        const int r = __ffs(b) - 1;
+        if (c - ps.r[r].s[axis] < ps.r[r].n[axis]) m |= 1u << r;
+    }
+    return m;
+}
+
 template <bool IDX>
 __device__ __forceinline__ void coeffs_f(const FusedGrid& g, size_t c, uint32_t m, int base, float out[6]) {
     if (IDX) {
@@ -382,74 +416,86 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
     const int lane = threadIdx.x;
     const uint32_t z0 = blockIdx.x * RZ;
     const int64_t zl = (int64_t)z0 + lane - 1;                  // this lane's z
-    const uint32_t zload = zl < 0 ? 0u : (uint32_t)zl;           // z = -1 loads z = 0 (self reference)
+    const uint32_t z = zl < 0 ? 0u : (uint32_t)zl;              // z = -1 reads z = 0 (self reference)
     const bool zin = zl < (int64_t)g.Nz;
     const bool own_z = lane >= 1 && lane <= RZ && zin;
     const uint32_t y0 = (blockIdx.y * blockDim.y + threadIdx.y) * RY;
     if (y0 >= g.Ny) return;                                      // whole warp idle (uniform per warp)
-    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
+    const size_t N = g.N, NyNz = g.NyNz;
+    const uint32_t Nz = g.Nz;
     const uint32_t xs = blockIdx.z * g.xchunk;
     if (xs >= g.Nx) return;
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
     const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;
-    const uint32_t z = (uint32_t)(zl < 0 ? 0 : zl);
-    uint32_t pmask = 0;
+    // UPML: candidate regions of this warp's box, then per-axis masks (cell mask = AND)
+    uint32_t zmask = 0, ymask[RY + 1];
+#pragma unroll
+    for (int r = 0; r <= RY; ++r) ymask[r] = 0;
+    uint32_t cand = 0;
     if (PML) {
-        const uint32_t lo[3] = {xs, y0 > 0 ? y0 - 1 : 0, z0 > 0 ? z0 - 1 : 0};
+        const uint32_t lo[3] = {xs, y0, z0 > 0 ? z0 - 1 : 0};
         const uint32_t hi[3] = {xe, y0 + RY, z0 + RZ};
-        pmask = region_mask(ps, lo, hi);
+        cand = region_mask(ps, lo, hi);
+        if (cand) {
+            zmask = axis_mask(ps, cand, 2, z);
+#pragma unroll
+            for (int r = 0; r <= RY; ++r) ymask[r] = axis_mask(ps, cand, 1, y0 + r);
+        }
     }
     bool rin[RY + 1];
 #pragma unroll
     for (int r = 0; r <= RY; ++r) rin[r] = (y0 + r < g.Ny) && zin;
     const uint32_t ym = y0 > 0 ? y0 - 1 : y0;                    // y = -1 reads y = 0 (self reference)
+    // per-thread offsets inside a plane
+    const size_t rowm = (size_t)ym * Nz + z;                     // the y-1 halo row
+    const size_t row0 = (size_t)y0 * Nz + z;
 
     float hp[RY + 1][3];     // H_old(x-1) rows y0..y0+RY
     float ep[RY + 1][3];     // E_new(x-1) rows y0..y0+RY
     uint32_t mp[RY];         // material rows of plane x-1 (owned rows)
+    uint32_t xmask_p = 0;    // UPML regions containing plane x-1
 #pragma unroll
     for (int r = 0; r <= RY; ++r) { hp[r][0] = hp[r][1] = hp[r][2] = 0.f; ep[r][0] = ep[r][1] = ep[r][2] = 0.f; }
 #pragma unroll
     for (int r = 0; r < RY; ++r) mp[r] = 0;
     if (xs > 0) {
-        const size_t b = (size_t)(xs - 1) * NyNz + zload;
+        const float* H = g.H0 + (size_t)(xs - 1) * NyNz + row0;
 #pragma unroll
         for (int r = 0; r <= RY; ++r)
             if (rin[r]) {
-                const size_t c = b + (size_t)(y0 + r) * Nz;
-                hp[r][1] = __ldg(g.H0 + N + c);
-                hp[r][2] = __ldg(g.H0 + 2 * N + c);
+                hp[r][1] = __ldg(H + N + (size_t)r * Nz);
+                hp[r][2] = __ldg(H + 2 * N + (size_t)r * Nz);
             }
     }
     for (uint32_t x = xs; x <= xl; ++x) {
-        const size_t bx = (size_t)x * NyNz + zload;
+        const size_t px = (size_t)x * NyNz;
+        const float* H = g.H0 + px;
+        const float* V = g.V0 + px;
+        const uint32_t xmask = cand ? axis_mask(ps, cand, 0, x) : 0u;
         // ---- loads of plane x: H rows y0-1..y0+RY, E_old and material rows y0..y0+RY
         float h[RY + 2][3], eo[RY + 1][3];
         uint32_t m[RY + 1];
-        {
-            const size_t c = bx + (size_t)ym * Nz;
-            h[0][0] = zin ? __ldg(g.H0 + c) : 0.f;
-            h[0][1] = 0.f;
-            h[0][2] = zin ? __ldg(g.H0 + 2 * N + c) : 0.f;
-        }
+        h[0][0] = zin ? __ldg(H + rowm) : 0.f;
+        h[0][1] = 0.f;
+        h[0][2] = zin ? __ldg(H + 2 * N + rowm) : 0.f;
 #pragma unroll
         for (int r = 0; r <= RY; ++r) {
-            const size_t c = bx + (size_t)(y0 + r) * Nz;
+            const size_t c = row0 + (size_t)r * Nz;
 #pragma unroll
             for (int n = 0; n < 3; ++n) {
-                h[r + 1][n] = rin[r] ? __ldg(g.H0 + n * N + c) : 0.f;
-                eo[r][n] = rin[r] ? __ldg(g.V0 + n * N + c) : 0.f;
+                h[r + 1][n] = rin[r] ? __ldg(H + n * N + c) : 0.f;
+                eo[r][n] = rin[r] ? __ldg(V + n * N + c) : 0.f;
             }
-            m[r] = (IDX && rin[r]) ? __ldg(g.mat + c) : 0u;
+            m[r] = (IDX && rin[r]) ? __ldg(g.mat + px + c) : 0u;
         }
-        uint32_t dbits[RY];
+        uint32_t dbits = 0;
+        if (g.defer && x > xs && own_z) {
 #pragma unroll
-        for (int r = 0; r < RY; ++r) {
-            dbits[r] = 0;
-            if (g.defer && x > xs && own_z && rin[r]) {
-                const size_t cm = (size_t)(x - 1) * NyNz + (size_t)(y0 + r) * Nz + z;
-                dbits[r] = (__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u;
-            }
+            for (int r = 0; r < RY; ++r)
+                if (rin[r]) {
+                    const size_t cm = px - NyNz + row0 + (size_t)r * Nz;
+                    dbits |= ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) << r;
+                }
         }
         const bool self = (x == 0);
         // ---- E_new(x) on rows y0..y0+RY (row RY is the y halo), lanes 1..31
@@ -465,14 +511,15 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
             const float cz = curl4(hy, hy_xm, hx, h[r][0]);
             en[r][0] = en[r][1] = en[r][2] = 0.f;
             if (lane >= 1 && rin[r]) {
-                const size_t c = bx + (size_t)(y0 + r) * Nz;
+                const size_t c = px + row0 + (size_t)r * Nz;
                 float kk[6];
                 coeffs_f<IDX>(g, c, m[r], 0, kk);
-                if (PML && pmask) {
+                const uint32_t cmask = zmask & ymask[r] & xmask;
+                if (PML && cmask) {
                     const bool wr = own_z && r < RY && x < xe;
-                    en[r][0] = pml_chain_pp<true>(ps, pn, pmask, x, y0 + r, z, 0, eo[r][0], true, kk[0], kk[3], cx, wr);
-                    en[r][1] = pml_chain_pp<true>(ps, pn, pmask, x, y0 + r, z, 1, eo[r][1], true, kk[1], kk[4], cy, wr);
-                    en[r][2] = pml_chain_pp<true>(ps, pn, pmask, x, y0 + r, z, 2, eo[r][2], true, kk[2], kk[5], cz, wr);
+                    en[r][0] = pml_cell<true>(ps, pn, cmask, x, y0 + r, z, 0, eo[r][0], true, kk[0], kk[3], cx, wr);
+                    en[r][1] = pml_cell<true>(ps, pn, cmask, x, y0 + r, z, 1, eo[r][1], true, kk[1], kk[4], cy, wr);
+                    en[r][2] = pml_cell<true>(ps, pn, cmask, x, y0 + r, z, 2, eo[r][2], true, kk[2], kk[5], cz, wr);
                 } else {
                     en[r][0] = upd(eo[r][0], kk[0], kk[3], cx);
                     en[r][1] = upd(eo[r][1], kk[1], kk[4], cy);
@@ -491,10 +538,10 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
             for (int r = 0; r < RY; ++r) {
                 const float ey_zp = __shfl_down_sync(0xffffffffu, ep[r][1], 1);
                 const float ex_zp = __shfl_down_sync(0xffffffffu, ep[r][0], 1);
-                if (!own_z || !rin[r] || dbits[r]) continue;
+                if (!own_z || !rin[r] || ((dbits >> r) & 1u)) continue;
                 const uint32_t y = y0 + r;
-                const size_t cm = (size_t)(x - 1) * NyNz + (size_t)y * Nz + z;
-                const bool core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
+                const size_t cm = px - NyNz + row0 + (size_t)r * Nz;
+                const bool core = (y + 1 < g.Ny) && (z + 1 < Nz);
                 float cx = 0.f, cy = 0.f, cz = 0.f;
                 float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 if (core) {
@@ -504,11 +551,12 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
                     coeffs_f<IDX>(g, cm, mp[r], 6, kk);
                 }
                 float hn[3];
-                if (PML && pmask) {
+                const uint32_t cmask = zmask & ymask[r] & xmask_p;
+                if (PML && cmask) {
 #pragma unroll
                     for (int n = 0; n < 3; ++n)
-                        hn[n] = pml_chain_pp<false>(ps, pn, pmask, x - 1, y, z, n, hp[r][n], core, kk[n], kk[3 + n],
-                                                    n == 0 ? cx : (n == 1 ? cy : cz), true);
+                        hn[n] = pml_cell<false>(ps, pn, cmask, x - 1, y, z, n, hp[r][n], core, kk[n], kk[3 + n],
+                                                n == 0 ? cx : (n == 1 ? cy : cz), true);
                 } else if (core) {
                     hn[0] = upd(hp[r][0], kk[0], kk[3], cx);
                     hn[1] = upd(hp[r][1], kk[1], kk[4], cy);
@@ -529,17 +577,19 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
         }
 #pragma unroll
         for (int r = 0; r < RY; ++r) mp[r] = m[r];
+        xmask_p = xmask;
     }
     // ---- H of the last plane x = Nx-1: no core update, UPML / pass-through only
     if (xe == g.Nx && own_z) {
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             if (!rin[r]) continue;
-            const size_t cm = (size_t)(g.Nx - 1) * NyNz + (size_t)(y0 + r) * Nz + z;
+            const size_t cm = (size_t)(g.Nx - 1) * NyNz + row0 + (size_t)r * Nz;
             if (g.defer && ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u)) continue;
+            const uint32_t cmask = zmask & ymask[r] & xmask_p;
 #pragma unroll
             for (int n = 0; n < 3; ++n)
-                g.H1[n * N + cm] = (PML && pmask) ? pml_chain_pp<false>(ps, pn, pmask, g.Nx - 1, y0 + r, z, n, hp[r][n], false, 0.f, 0.f, 0.f, true)
+                g.H1[n * N + cm] = (PML && cmask) ? pml_cell<false>(ps, pn, cmask, g.Nx - 1, y0 + r, z, n, hp[r][n], false, 0.f, 0.f, 0.f, true)
                                                   : hp[r][n];
         }
     }

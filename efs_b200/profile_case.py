@@ -15,6 +15,7 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--time-core", type=int, default=0, help="also time N launches of the core kernel(s) alone")
     args = ap.parse_args()
     from efs_b200.build import build
     build()
@@ -32,8 +33,13 @@ def main():
     eng.sync()
     dt = (time.perf_counter() - t) / max(1, args.steps)
     N = args.n ** 3
-    print("n=%d steps=%d  %.3f ms/timestep  %.1f MCells/s  kernels/step=%d" %
-          (args.n, args.steps, dt * 1e3, N / dt / 1e6, eng.kernelsPerStep()))
+    line = "n=%d steps=%d  %.3f ms/timestep  %.1f MCells/s  kernels/step=%d" % (
+        args.n, args.steps, dt * 1e3, N / dt / 1e6, eng.kernelsPerStep())
+    if args.time_core:
+        ms = eng.timeCore(args.time_core)
+        core = ms[0] + ms[1]
+        line += "  core %.3f ms (%.0f GB/s at 52 B/cell)" % (core, 52.0 * N / (core / 1e3) / 1e9)
+    print(line)
     eng.destroy()
 
 
