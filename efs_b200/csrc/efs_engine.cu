@@ -21,8 +21,10 @@
 #include "../../include/efs.h"
 #include "efs_kernels.cuh"
 #include "efs_fused.cuh"
+#include "efs_tma.cuh"
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -91,9 +93,9 @@ struct efs_engine {
     uint32_t xchunk = 64;       // x-planes per block of the fused kernel
     int cpt = 1;                // z cells per thread of the fused kernel (1 or 2)
     int ty_rows = 8;            // y rows per tile of the shared-memory fused kernel (8 or 16)
-    int fused_kind = 0;         // 0: register-blocked fused kernel, 1: shared-memory tiled fused kernel
+    int fused_kind = 2;         // 2: TMA-fed fused kernel (needs Nz % 4 == 0, else 0), 0: register-blocked, 1: shared-memory tiled
     int ry = 4;                 // y rows per thread of the register-blocked kernel (2, 4, 8)
-    DevBuf defer_bits, defer_cells;
+    DevBuf defer_bits, defer_rows, defer_cells;
     uint32_t defer_n = 0;
     std::vector<uint32_t> h_exc_targets, h_tfsf_v_targets, h_mur_apply, h_rlc_series;
     bool indexed = false;
@@ -181,6 +183,9 @@ struct efs_engine {
     // energy (lagged, double-buffered like computeEnergy :2974-3021)
     DevBuf en_partial, en_result;
     double* en_host = nullptr;       // pinned, 2 slots
+    // device status word in mapped pinned host memory: bit 0 = a bounded device wait ran out
+    uint32_t* h_status = nullptr;
+    uint32_t* d_status = nullptr;
     cudaEvent_t en_event[2] = {nullptr, nullptr};
     int en_idx = 0;
     bool en_pending = false;
@@ -194,6 +199,7 @@ struct efs_engine {
         drop_graphs();
         for (auto& ev : en_event) if (ev) cudaEventDestroy(ev);
         if (en_host) cudaFreeHost(en_host);
+        if (h_status) cudaFreeHost(h_status);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -214,10 +220,20 @@ struct efs_engine {
     void upload(DevBuf& b, const T* src, size_t n) {
         alloc(b, n * sizeof(T), false);
         if (n) ck(cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
-        ck(cudaStreamSynchronize(stream), "upload sync");   // caller may free its buffer on return
+        sync("upload sync");   // caller may free its buffer on return
     }
     template <typename T>
     void upload(DevBuf& b, const std::vector<T>& v) { upload(b, v.data(), v.size()); }
+
+    // Synchronize the stream and turn a device status report into an error.
+    void sync(const char* what) {
+        ck(cudaStreamSynchronize(stream), what);
+        const uint32_t st = *(volatile uint32_t*)h_status;
+        if (st) {
+            *(volatile uint32_t*)h_status = 0;
+            fail(EFS_ERR_TIMEOUT, std::string(what) + ": a bounded device wait for a TMA plane load ran out");
+        }
+    }
 
     void need_init() const { if (!inited) fail(EFS_ERR_STATE, "engine not initialised: call efs_init first"); }
     void check_idx3(const uint32_t* p, size_t n, const char* what) const {
@@ -242,6 +258,8 @@ struct efs_engine {
         g.mat = mat.as<uint32_t>(); g.table = table.as<float>();
         g.vv = vv.as<float>(); g.vi = vi.as<float>(); g.ii = ii.as<float>(); g.iv = iv.as<float>();
         g.defer = defer_n ? defer_bits.as<uint32_t>() : nullptr;
+        g.defer_rows = defer_n ? defer_rows.as<uint32_t>() : nullptr;
+        g.status = d_status;
         return g;
     }
     // UPML set whose flux pointers are the parity-p buffers
@@ -353,6 +371,15 @@ struct efs_engine {
         std::vector<uint32_t> cells;
         for (size_t w = 0; w < bits.size(); ++w)
             for (uint32_t b = bits[w]; b; b &= b - 1) cells.push_back((uint32_t)(w * 32 + __builtin_ctz(b)));
+        // row summary: bit y of plane x set when row (x, y) holds a deferred cell
+        const uint32_t rw = (Ny + 31) / 32;
+        std::vector<uint32_t> rows((size_t)Nx * rw, 0);
+        for (uint32_t c : cells) {
+            const size_t xy = c / Nz;
+            const uint32_t x = (uint32_t)(xy / Ny), y = (uint32_t)(xy % Ny);
+            rows[(size_t)x * rw + (y >> 5)] |= 1u << (y & 31);
+        }
+        upload(defer_rows, rows);
         upload(defer_bits, bits);
         upload(defer_cells, cells);
         defer_n = (uint32_t)cells.size();
@@ -449,17 +476,69 @@ struct efs_engine {
         if (indexed) { if (hp) launch_fused_k<true, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<true, false, CPT, TY>(g, b, fg, ps, pn); }
         else { if (hp) launch_fused_k<false, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<false, false, CPT, TY>(g, b, fg, ps, pn); }
     }
+    template <int RY, typename IT>
+    void launch_fused_reg_k(dim3 g, dim3 b, const FusedGrid& fg, const PmlSet& ps, const PmlSet& pn) {
+        const bool hp = !pml.empty();
+        if (indexed) { if (hp) k_fused_reg<true, true, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<true, false, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); }
+        else { if (hp) k_fused_reg<false, true, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<false, false, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); }
+    }
     template <int RY>
     void launch_fused_reg(int p) {
         const FusedGrid fg = fused_grid(p);
         const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
         dim3 b(32, 4), g(blocks(Nz, RZ), blocks(Ny, 4 * RY), blocks(Nx, xchunk));
+        launch_fused_reg_k<RY, uint32_t>(g, b, fg, ps, pn);   // efs_init guarantees 3*N < 2^32
+    }
+    // TMA-fed kernel: tensor maps over this parity's fields and the material
+    // rows, boxes of one tile plus halos (efs_tma.cuh)
+    CUtensorMap tensor_map(const void* base, CUtensorMapDataType dt, uint32_t rank, const uint32_t box[4]) const {
+        static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+        if (!encode) {
+            void* fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
+            if (q != cudaDriverEntryPointSuccess || !fn) fail(EFS_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        }
+        const cuuint64_t dims[4] = {Nz, Ny, Nx, 3};
+        const cuuint64_t strides[3] = {(cuuint64_t)Nz * 4, (cuuint64_t)Ny * Nz * 4, (cuuint64_t)N * 4};
+        const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+        const cuuint32_t es[4] = {1, 1, 1, 1};
+        CUtensorMap m;
+        const CUresult r = encode(&m, dt, rank, const_cast<void*>(base), dims, strides, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) fail(EFS_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
+        return m;
+    }
+    template <bool IDX, bool PML>
+    void launch_fused_tma_k(dim3 g, const CUtensorMap& tH, const CUtensorMap& tE, const CUtensorMap& tM, const FusedGrid& fg,
+                            const PmlSet& ps, const PmlSet& pn) {
+        static bool attr_set = false;   // per instantiation; the attribute is per kernel, all devices alike
+        if (!attr_set) {
+            ck(cudaFuncSetAttribute(k_fused_tma<IDX, PML>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT_SMEM_BYTES),
+               "smem attr");
+            attr_set = true;
+        }
+        k_fused_tma<IDX, PML><<<g, TT_THREADS, TT_SMEM_BYTES, stream>>>(tH, tE, tM, fg, ps, pn);
+    }
+    void launch_fused_tma(int p) {
+        const FusedGrid fg = fused_grid(p);
+        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
+        const uint32_t bh[4] = {TT_HZ, TT_HY, 1, 3}, be[4] = {TT_EZ, TT_EY, 1, 3};
+        const CUtensorMap tH = tensor_map(fg.H0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, bh);
+        const CUtensorMap tE = tensor_map(fg.V0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, be);
+        const CUtensorMap tM = indexed ? tensor_map(fg.mat, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, be) : tE;
+        dim3 g(blocks(Nz, TT_Z), blocks(Ny, TT_Y), blocks(Nx, xchunk));
         const bool hp = !pml.empty();
-        if (indexed) { if (hp) k_fused_reg<true, true, RY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<true, false, RY><<<g, b, 0, stream>>>(fg, ps, pn); }
-        else { if (hp) k_fused_reg<false, true, RY><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<false, false, RY><<<g, b, 0, stream>>>(fg, ps, pn); }
+        if (indexed) { if (hp) launch_fused_tma_k<true, true>(g, tH, tE, tM, fg, ps, pn); else launch_fused_tma_k<true, false>(g, tH, tE, tM, fg, ps, pn); }
+        else { if (hp) launch_fused_tma_k<false, true>(g, tH, tE, tM, fg, ps, pn); else launch_fused_tma_k<false, false>(g, tH, tE, tM, fg, ps, pn); }
     }
     void launch_fused(int p) {
-        if (fused_kind == 0) {
+        if (fused_kind == 2 && Nz % 4 == 0) {
+            launch_fused_tma(p);
+            return;
+        }
+        if (fused_kind != 1) {
             if (ry >= 8) launch_fused_reg<8>(p);
             else if (ry >= 4) launch_fused_reg<4>(p);
             else launch_fused_reg<2>(p);
@@ -543,7 +622,7 @@ struct efs_engine {
     void sync_state_to_device() {
         hstate.numTS = numTS;
         ck(cudaMemcpyAsync(state.p, &hstate, sizeof(StepState), cudaMemcpyHostToDevice, stream), "state upload");
-        ck(cudaStreamSynchronize(stream), "state sync");
+        sync("state sync");
     }
 
     // group entries by target preserving order: returns unique targets + CSR offsets + permutation
@@ -598,7 +677,8 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     if (const char* s = getenv("EFS_XCHUNK")) e->xchunk = std::max(1, atoi(s));
     if (const char* s = getenv("EFS_CPT")) e->cpt = std::max(1, atoi(s));
     if (const char* s = getenv("EFS_TY")) e->ty_rows = std::max(8, atoi(s));
-    if (const char* s = getenv("EFS_FUSED")) e->fused_kind = std::string(s) == "smem" ? 1 : 0;
+    e->fused_kind = 2;
+    if (const char* s = getenv("EFS_FUSED")) e->fused_kind = std::string(s) == "smem" ? 1 : std::string(s) == "reg" ? 0 : 2;
     if (const char* s = getenv("EFS_RY")) e->ry = std::max(2, atoi(s));
     e->cur = 0;
     e->alloc(e->volt, 3 * N * sizeof(float));
@@ -647,6 +727,9 @@ efs_status efs_create(efs_engine** out, int device) {
         ck(cudaSetDevice(device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaMallocHost(&e->en_host, 2 * sizeof(double)), "cudaMallocHost");
+        ck(cudaHostAlloc(&e->h_status, sizeof(uint32_t), cudaHostAllocMapped), "cudaHostAlloc");
+        *e->h_status = 0;
+        ck(cudaHostGetDevicePointer(&e->d_status, e->h_status, 0), "cudaHostGetDevicePointer");
         for (auto& ev : e->en_event) ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
     } catch (const EfsError& ex) {
         g_create_error = ex.msg;
@@ -980,7 +1063,7 @@ efs_status efs_read_steady_state(efs_engine* e, float* e1, float* e2, uint32_t* 
         std::vector<float> a(e->ss_n), b(e->ss_n);
         ck(cudaMemcpyAsync(a.data(), e->ss_e1.p, (size_t)e->ss_n * 4, cudaMemcpyDeviceToHost, e->stream), "read ss");
         ck(cudaMemcpyAsync(b.data(), e->ss_e2.p, (size_t)e->ss_n * 4, cudaMemcpyDeviceToHost, e->stream), "read ss");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
         uint32_t sample = e->ss_count_before + (e->ss_recording ? e->numTS - e->hstate.ss_start : 0);
         if (e1) memcpy(e1, a.data(), a.size() * 4);
         if (e2) memcpy(e2, b.data(), b.size() * 4);
@@ -1010,7 +1093,7 @@ efs_status efs_num_ts(const efs_engine* e, uint32_t* out) {
     return EFS_OK;
 }
 
-efs_status efs_sync(efs_engine* e) { return guard(e, [&] { ck(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize"); }); }
+efs_status efs_sync(efs_engine* e) { return guard(e, [&] { e->sync("cudaStreamSynchronize"); }); }
 
 efs_status efs_get_stream(efs_engine* e, void** s) {
     if (!e || !s) return EFS_ERR_INVALID;
@@ -1039,7 +1122,7 @@ efs_status efs_read_probe_gather(efs_engine* e, float* out, size_t len) {
                                                              e->gd_n, e->gd_out.as<float>());
         ck(cudaGetLastError(), "gather");
         ck(cudaMemcpyAsync(out, e->gd_out.p, 2 * (size_t)e->gd_n * 4, cudaMemcpyDeviceToHost, e->stream), "read gather");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1071,7 +1154,7 @@ efs_status efs_read_probe_gather_buffered(efs_engine* e, float* out, size_t len,
         size_t need = (size_t)s * e->ring_n * 2;
         if (len < need) fail(EFS_ERR_INVALID, "output buffer too small");
         if (need) ck(cudaMemcpyAsync(out, e->ring.p, need * 4, cudaMemcpyDeviceToHost, e->stream), "read ring");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1120,7 +1203,7 @@ efs_status efs_read_nf2ff(efs_engine* e, float* accE, float* accH, size_t len) {
         if (len < n) fail(EFS_ERR_INVALID, "output buffer too small");
         if (accE) ck(cudaMemcpyAsync(accE, e->nf_E.p, n * 4, cudaMemcpyDeviceToHost, e->stream), "read nf2ff E");
         if (accH) ck(cudaMemcpyAsync(accH, e->nf_H.p, n * 4, cudaMemcpyDeviceToHost, e->stream), "read nf2ff H");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1161,7 +1244,7 @@ efs_status efs_far_field(efs_engine* e, uint32_t fi, const float* meta, const fl
                                                                    fmag * std::cos(fph), dout.as<float>());
         ck(cudaGetLastError(), "far field");
         ck(cudaMemcpyAsync(out, dout.p, (size_t)A * 5 * 4, cudaMemcpyDeviceToHost, e->stream), "read far field");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1223,7 +1306,7 @@ efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
         e->need_init();
         if (v) ck(cudaMemcpyAsync(v, e->vcur(), 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read volt");
         if (c) ck(cudaMemcpyAsync(c, e->ccur(), 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read curr");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1232,7 +1315,7 @@ efs_status efs_set_fields(efs_engine* e, const float* v, const float* c) {
         e->need_init();
         if (v) ck(cudaMemcpyAsync(e->vcur(), v, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write volt");
         if (c) ck(cudaMemcpyAsync(e->ccur(), c, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write curr");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1271,7 +1354,7 @@ efs_status efs_get_state(efs_engine* e, void* buf, size_t cap, size_t* size) {
             ck(cudaMemcpyAsync(p, d->p, d->bytes, cudaMemcpyDeviceToHost, e->stream), "state read");
             p += d->bytes;
         }
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
     });
 }
 
@@ -1295,7 +1378,7 @@ efs_status efs_set_state(efs_engine* e, const void* buf, size_t size) {
             ck(cudaMemcpyAsync(d->p, p, nb, cudaMemcpyHostToDevice, e->stream), "state write");
             p += nb;
         }
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
         e->numTS = (uint32_t)hdr[2];
         e->sync_state_to_device();
     });
@@ -1328,7 +1411,7 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
         if (cap < n) fail(EFS_ERR_INVALID, "output buffer too small");
         std::vector<float> tmp(n);
         if (n) ck(cudaMemcpyAsync(tmp.data(), b->p, n * 4, cudaMemcpyDeviceToHost, e->stream), "debug read");
-        ck(cudaStreamSynchronize(e->stream), "sync");
+        e->sync("sync");
         if (s.rfind("rlc_", 0) == 0) {
             // device keeps elements grouped by field cell; restore caller order
             const size_t w = (s == "rlc_vil") ? 1 : 3;
@@ -1362,6 +1445,7 @@ efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms) {
             float a = 0;
             cudaEventElapsedTime(&a, ev[0], ev[1]);
             for (auto& x : ev) cudaEventDestroy(x);
+            e->sync("fused timing");
             ms[0] = a / reps;
             ms[1] = 0.f;
             return;
@@ -1406,7 +1490,7 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
 efs_status efs_device_bytes(const efs_engine* e, size_t* out) {
     if (!e || !out) return EFS_ERR_INVALID;
     size_t t = 0;
-    const DevBuf* all[] = {&e->volt, &e->curr, &e->volt_b, &e->curr_b, &e->defer_bits, &e->defer_cells, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
+    const DevBuf* all[] = {&e->volt, &e->curr, &e->volt_b, &e->curr_b, &e->defer_bits, &e->defer_rows, &e->defer_cells, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
     for (auto* b : all) t += b->bytes;
     for (auto& r : e->pml) {
         const DevBuf* rb[] = {&r->vv, &r->vvfo, &r->vvfn, &r->ii, &r->iifo, &r->iifn, &r->vflux, &r->cflux, &r->vflux_b, &r->cflux_b};

@@ -34,6 +34,8 @@ struct FusedGrid {
     const uint32_t* mat; const float* table;
     const float* vv; const float* vi; const float* ii; const float* iv;
     const uint32_t* defer;              // bit per cell: H update deferred (may be null)
+    const uint32_t* defer_rows;         // bit per (x, y) row holding a deferred cell; ceil(Ny/32) words per x
+    uint32_t* status;                   // device status word (bit 0: a bounded wait ran out)
 };
 
 // UPML chain with separate old/new flux buffers; up to PML_MAX_OVERLAP regions per cell.
@@ -109,9 +111,15 @@ __device__ __forceinline__ uint32_t axis_mask(const PmlSet& ps, uint32_t cand, i
 template <bool IDX>
 __device__ __forceinline__ void coeffs_f(const FusedGrid& g, size_t c, uint32_t m, int base, float out[6]) {
     if (IDX) {
-        const float* t = g.table + (size_t)m * 12 + base;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) out[k] = __ldg(t + k);
+        // a 48-byte row is three float4: [vv0 vv1 vv2 vi0][vi1 vi2 ii0 ii1][ii2 iv0 iv1 iv2]
+        const float4* t = reinterpret_cast<const float4*>(g.table) + (size_t)m * 3;
+        if (base == 0) {
+            const float4 a = __ldg(t), b = __ldg(t + 1);
+            out[0] = a.x; out[1] = a.y; out[2] = a.z; out[3] = a.w; out[4] = b.x; out[5] = b.y;
+        } else {
+            const float4 b = __ldg(t + 1), d = __ldg(t + 2);
+            out[0] = b.z; out[1] = b.w; out[2] = d.x; out[3] = d.y; out[4] = d.z; out[5] = d.w;
+        }
     } else {
         const float* a = base == 0 ? g.vv : g.ii;
         const float* b = base == 0 ? g.vi : g.iv;
@@ -408,11 +416,21 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k_fused(const FusedGrid g, cons
 // is the y halo) and keeps the previous plane's H_old and E_new in registers
 // while it streams x.  Every warp is independent, so the SM keeps many
 // planes' loads in flight.
+//
+// A warp-plane whose rows and lanes all lie inside the grid and which no UPML
+// region reaches (most of a large grid) runs a branch-free body; the others
+// run the general body with per-cell range checks and the UPML chain.  IT is
+// the index type: 32-bit whenever 3*N fits, so that an access costs one
+// multiply-add of address arithmetic.
 // ---------------------------------------------------------------------------
 constexpr int RZ = 30;          // owned z per warp
 
-template <bool IDX, bool PML, int RY>
+template <bool B>
+struct PlaneKind { static constexpr bool value = B; };
+
+template <bool IDX, bool PML, int RY, typename IT>
 __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlSet ps, const PmlSet pn) {
+    static_assert(32 % RY == 0, "the RY rows of a thread share one word of the row summary");
     const int lane = threadIdx.x;
     const uint32_t z0 = blockIdx.x * RZ;
     const int64_t zl = (int64_t)z0 + lane - 1;                  // this lane's z
@@ -421,102 +439,100 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
     const bool own_z = lane >= 1 && lane <= RZ && zin;
     const uint32_t y0 = (blockIdx.y * blockDim.y + threadIdx.y) * RY;
     if (y0 >= g.Ny) return;                                      // whole warp idle (uniform per warp)
-    const size_t N = g.N, NyNz = g.NyNz;
-    const uint32_t Nz = g.Nz;
     const uint32_t xs = blockIdx.z * g.xchunk;
     if (xs >= g.Nx) return;
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
     const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;
+    const IT N = (IT)g.N, NyNz = (IT)g.NyNz, Nz = (IT)g.Nz;
+    // rows y0..y0+RY and lanes z0-1..z0+30 all inside the grid, every owned H cell with its full curl
+    const bool inner = (y0 + RY < g.Ny) && (z0 + RZ < g.Nz);
     // UPML: candidate regions of this warp's box, then per-axis masks (cell mask = AND)
     uint32_t zmask = 0, ymask[RY + 1];
 #pragma unroll
     for (int r = 0; r <= RY; ++r) ymask[r] = 0;
-    uint32_t cand = 0;
+    uint32_t cand = 0, zy = 0;
     if (PML) {
         const uint32_t lo[3] = {xs, y0, z0 > 0 ? z0 - 1 : 0};
         const uint32_t hi[3] = {xe, y0 + RY, z0 + RZ};
         cand = region_mask(ps, lo, hi);
-        if (cand) {
+        if (cand) {                                              // uniform per warp
             zmask = axis_mask(ps, cand, 2, z);
+            uint32_t yu = 0;
 #pragma unroll
-            for (int r = 0; r <= RY; ++r) ymask[r] = axis_mask(ps, cand, 1, y0 + r);
+            for (int r = 0; r <= RY; ++r) { ymask[r] = axis_mask(ps, cand, 1, y0 + r); yu |= ymask[r]; }
+            zy = __reduce_or_sync(0xffffffffu, zmask) & yu;     // regions meeting the warp's (y, z) footprint
         }
     }
     bool rin[RY + 1];
 #pragma unroll
     for (int r = 0; r <= RY; ++r) rin[r] = (y0 + r < g.Ny) && zin;
     const uint32_t ym = y0 > 0 ? y0 - 1 : y0;                    // y = -1 reads y = 0 (self reference)
-    // per-thread offsets inside a plane
-    const size_t rowm = (size_t)ym * Nz + z;                     // the y-1 halo row
-    const size_t row0 = (size_t)y0 * Nz + z;
+    const IT rowm = (IT)ym * Nz + z;                             // offsets inside a plane: the y-1 halo row
+    const IT row0 = (IT)y0 * Nz + z;                             //   and row y0
+    const uint32_t rw = (g.Ny + 31) / 32;                        // words per plane of the row summary
 
     float hp[RY + 1][3];     // H_old(x-1) rows y0..y0+RY
     float ep[RY + 1][3];     // E_new(x-1) rows y0..y0+RY
     uint32_t mp[RY];         // material rows of plane x-1 (owned rows)
-    uint32_t xmask_p = 0;    // UPML regions containing plane x-1
 #pragma unroll
     for (int r = 0; r <= RY; ++r) { hp[r][0] = hp[r][1] = hp[r][2] = 0.f; ep[r][0] = ep[r][1] = ep[r][2] = 0.f; }
 #pragma unroll
     for (int r = 0; r < RY; ++r) mp[r] = 0;
-    if (xs > 0) {
-        const float* H = g.H0 + (size_t)(xs - 1) * NyNz + row0;
+    {   // H_old(xs-1); at xs = 0 the x-1 neighbour is plane 0 itself (self reference)
+        const float* H = g.H0 + (IT)(xs > 0 ? xs - 1 : 0) * NyNz;
 #pragma unroll
         for (int r = 0; r <= RY; ++r)
             if (rin[r]) {
-                hp[r][1] = __ldg(H + N + (size_t)r * Nz);
-                hp[r][2] = __ldg(H + 2 * N + (size_t)r * Nz);
+                const IT c = row0 + (IT)r * Nz;
+                hp[r][1] = __ldg(H + (c + N));
+                hp[r][2] = __ldg(H + (c + 2 * N));
             }
     }
-    for (uint32_t x = xs; x <= xl; ++x) {
-        const size_t px = (size_t)x * NyNz;
+
+    // One plane: E_new(x) on rows y0..y0+RY (row RY is the y halo), then H_new(x-1) on the owned rows.
+    auto plane = [&](uint32_t x, uint32_t xmask, uint32_t xmask_p, auto kind) {
+        constexpr bool FAST = decltype(kind)::value;
+        const IT px = (IT)x * NyNz;
         const float* H = g.H0 + px;
         const float* V = g.V0 + px;
-        const uint32_t xmask = cand ? axis_mask(ps, cand, 0, x) : 0u;
+        const uint32_t* M = g.mat + px;
+        float* V1 = g.V1 + px;
         // ---- loads of plane x: H rows y0-1..y0+RY, E_old and material rows y0..y0+RY
         float h[RY + 2][3], eo[RY + 1][3];
         uint32_t m[RY + 1];
-        h[0][0] = zin ? __ldg(H + rowm) : 0.f;
+        h[0][0] = (FAST || zin) ? __ldg(H + rowm) : 0.f;
         h[0][1] = 0.f;
-        h[0][2] = zin ? __ldg(H + 2 * N + rowm) : 0.f;
+        h[0][2] = (FAST || zin) ? __ldg(H + (rowm + 2 * N)) : 0.f;
 #pragma unroll
         for (int r = 0; r <= RY; ++r) {
-            const size_t c = row0 + (size_t)r * Nz;
+            const IT c = row0 + (IT)r * Nz;
+            const bool ok = FAST || rin[r];
 #pragma unroll
             for (int n = 0; n < 3; ++n) {
-                h[r + 1][n] = rin[r] ? __ldg(H + n * N + c) : 0.f;
-                eo[r][n] = rin[r] ? __ldg(V + n * N + c) : 0.f;
+                h[r + 1][n] = ok ? __ldg(H + (c + n * N)) : 0.f;
+                eo[r][n] = ok ? __ldg(V + (c + n * N)) : 0.f;
             }
-            m[r] = (IDX && rin[r]) ? __ldg(g.mat + px + c) : 0u;
+            m[r] = (IDX && ok) ? __ldg(M + c) : 0u;
         }
-        uint32_t dbits = 0;
-        if (g.defer && x > xs && own_z) {
-#pragma unroll
-            for (int r = 0; r < RY; ++r)
-                if (rin[r]) {
-                    const size_t cm = px - NyNz + row0 + (size_t)r * Nz;
-                    dbits |= ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) << r;
-                }
-        }
-        const bool self = (x == 0);
-        // ---- E_new(x) on rows y0..y0+RY (row RY is the y halo), lanes 1..31
+        // ---- E_new(x)
         float en[RY + 1][3];
+        const bool store_e = x < xe;
 #pragma unroll
         for (int r = 0; r <= RY; ++r) {
+            const IT c = row0 + (IT)r * Nz;
             const float hx = h[r + 1][0], hy = h[r + 1][1], hz = h[r + 1][2];
             const float hy_zm = __shfl_up_sync(0xffffffffu, hy, 1);
             const float hx_zm = __shfl_up_sync(0xffffffffu, hx, 1);
-            const float hy_xm = self ? hy : hp[r][1], hz_xm = self ? hz : hp[r][2];
             const float cx = curl4(hz, h[r][2], hy, hy_zm);
-            const float cy = curl4(hx, hx_zm, hz, hz_xm);
-            const float cz = curl4(hy, hy_xm, hx, h[r][0]);
+            const float cy = curl4(hx, hx_zm, hz, hp[r][2]);
+            const float cz = curl4(hy, hp[r][1], hx, h[r][0]);
             en[r][0] = en[r][1] = en[r][2] = 0.f;
-            if (lane >= 1 && rin[r]) {
-                const size_t c = px + row0 + (size_t)r * Nz;
+            if (FAST || (lane >= 1 && rin[r])) {
                 float kk[6];
-                coeffs_f<IDX>(g, c, m[r], 0, kk);
-                const uint32_t cmask = zmask & ymask[r] & xmask;
+                coeffs_f<IDX>(g, (size_t)(px + c), m[r], 0, kk);
+                const uint32_t cmask = FAST ? 0u : (zmask & ymask[r] & xmask);
                 if (PML && cmask) {
-                    const bool wr = own_z && r < RY && x < xe;
+                    const bool wr = own_z && r < RY && store_e;
                     en[r][0] = pml_cell<true>(ps, pn, cmask, x, y0 + r, z, 0, eo[r][0], true, kk[0], kk[3], cx, wr);
                     en[r][1] = pml_cell<true>(ps, pn, cmask, x, y0 + r, z, 1, eo[r][1], true, kk[1], kk[4], cy, wr);
                     en[r][2] = pml_cell<true>(ps, pn, cmask, x, y0 + r, z, 2, eo[r][2], true, kk[2], kk[5], cz, wr);
@@ -525,30 +541,61 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
                     en[r][1] = upd(eo[r][1], kk[1], kk[4], cy);
                     en[r][2] = upd(eo[r][2], kk[2], kk[5], cz);
                 }
-                if (own_z && r < RY && x < xe) {
-                    g.V1[c] = en[r][0];
-                    g.V1[N + c] = en[r][1];
-                    g.V1[2 * N + c] = en[r][2];
+                if (own_z && r < RY && store_e) {
+                    V1[c] = en[r][0];
+                    V1[c + N] = en[r][1];
+                    V1[c + 2 * N] = en[r][2];
                 }
             }
         }
         // ---- H_new(x-1) on owned rows and lanes
         if (x > xs) {
+            const IT pm = px - NyNz;
+            float* H1 = g.H1 + pm;
+            uint32_t dbits = 0;                                  // rows whose cell is deferred
+            if (g.defer_rows) {
+                const uint32_t w = __ldg(g.defer_rows + (size_t)(x - 1) * rw + (y0 >> 5));
+                const uint32_t rows = (w >> (y0 & 31)) & ((1u << RY) - 1u);
+                if (rows && own_z) {
+#pragma unroll
+                    for (int r = 0; r < RY; ++r)
+                        if (((rows >> r) & 1u) && rin[r]) {
+                            const IT cm = pm + row0 + (IT)r * Nz;
+                            dbits |= ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u) << r;
+                        }
+                }
+            }
 #pragma unroll
             for (int r = 0; r < RY; ++r) {
+                const IT c = row0 + (IT)r * Nz;
                 const float ey_zp = __shfl_down_sync(0xffffffffu, ep[r][1], 1);
                 const float ex_zp = __shfl_down_sync(0xffffffffu, ep[r][0], 1);
+                if (FAST) {
+                    const float cx = curl4(ep[r][2], ep[r + 1][2], ep[r][1], ey_zp);
+                    const float cy = curl4(ep[r][0], ex_zp, ep[r][2], en[r][2]);
+                    const float cz = curl4(ep[r][1], en[r][1], ep[r][0], ep[r + 1][0]);
+                    float kk[6];
+                    coeffs_f<IDX>(g, (size_t)(pm + c), mp[r], 6, kk);
+                    const float h0 = upd(hp[r][0], kk[0], kk[3], cx);
+                    const float h1 = upd(hp[r][1], kk[1], kk[4], cy);
+                    const float h2 = upd(hp[r][2], kk[2], kk[5], cz);
+                    if (own_z && !((dbits >> r) & 1u)) {
+                        H1[c] = h0;
+                        H1[c + N] = h1;
+                        H1[c + 2 * N] = h2;
+                    }
+                    continue;
+                }
                 if (!own_z || !rin[r] || ((dbits >> r) & 1u)) continue;
                 const uint32_t y = y0 + r;
-                const size_t cm = px - NyNz + row0 + (size_t)r * Nz;
-                const bool core = (y + 1 < g.Ny) && (z + 1 < Nz);
+                const bool core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
                 float cx = 0.f, cy = 0.f, cz = 0.f;
                 float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 if (core) {
                     cx = curl4(ep[r][2], ep[r + 1][2], ep[r][1], ey_zp);
                     cy = curl4(ep[r][0], ex_zp, ep[r][2], en[r][2]);
                     cz = curl4(ep[r][1], en[r][1], ep[r][0], ep[r + 1][0]);
-                    coeffs_f<IDX>(g, cm, mp[r], 6, kk);
+                    coeffs_f<IDX>(g, (size_t)(pm + c), mp[r], 6, kk);
                 }
                 float hn[3];
                 const uint32_t cmask = zmask & ymask[r] & xmask_p;
@@ -564,9 +611,9 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
                 } else {
                     hn[0] = hp[r][0]; hn[1] = hp[r][1]; hn[2] = hp[r][2];
                 }
-                g.H1[cm] = hn[0];
-                g.H1[N + cm] = hn[1];
-                g.H1[2 * N + cm] = hn[2];
+                H1[c] = hn[0];
+                H1[c + N] = hn[1];
+                H1[c + 2 * N] = hn[2];
             }
         }
         // ---- rotate
@@ -577,19 +624,27 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
         }
 #pragma unroll
         for (int r = 0; r < RY; ++r) mp[r] = m[r];
+    };
+
+    uint32_t xmask_p = 0;    // UPML regions containing plane x-1
+    for (uint32_t x = xs; x <= xl; ++x) {
+        const uint32_t xmask = cand ? axis_mask(ps, cand, 0, x) : 0u;
+        if (inner && !(zy & (xmask | xmask_p))) plane(x, xmask, xmask_p, PlaneKind<true>{});
+        else plane(x, xmask, xmask_p, PlaneKind<false>{});
         xmask_p = xmask;
     }
     // ---- H of the last plane x = Nx-1: no core update, UPML / pass-through only
     if (xe == g.Nx && own_z) {
+        const IT pl = (IT)(g.Nx - 1) * NyNz;
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             if (!rin[r]) continue;
-            const size_t cm = (size_t)(g.Nx - 1) * NyNz + row0 + (size_t)r * Nz;
+            const IT cm = pl + row0 + (IT)r * Nz;
             if (g.defer && ((__ldg(g.defer + (cm >> 5)) >> (cm & 31)) & 1u)) continue;
             const uint32_t cmask = zmask & ymask[r] & xmask_p;
 #pragma unroll
             for (int n = 0; n < 3; ++n)
-                g.H1[n * N + cm] = (PML && cmask) ? pml_cell<false>(ps, pn, cmask, g.Nx - 1, y0 + r, z, n, hp[r][n], false, 0.f, 0.f, 0.f, true)
+                g.H1[cm + n * N] = (PML && cmask) ? pml_cell<false>(ps, pn, cmask, g.Nx - 1, y0 + r, z, n, hp[r][n], false, 0.f, 0.f, 0.f, true)
                                                   : hp[r][n];
         }
     }
