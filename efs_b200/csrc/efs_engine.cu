@@ -415,7 +415,9 @@ struct efs_engine {
             // ADE(curr) reads H and the current flux, which the E side never
             // touches: it runs before the fused kernel overwrites the flux.
             if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            if (pml_split()) launch_pml_e(p);
             launch_fused(p);
+            if (pml_split()) launch_pml_h(p);
         } else {
             dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
             if (indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, stream>>>(g, ps); }
@@ -512,29 +514,51 @@ struct efs_engine {
     }
     template <bool IDX, bool PML>
     void launch_fused_tma_k(dim3 g, const CUtensorMap& tH, const CUtensorMap& tE, const CUtensorMap& tM, const FusedGrid& fg,
-                            const PmlSet& ps, const PmlSet& pn) {
+                            const PmlSet& ps) {
         static bool attr_set = false;   // per instantiation; the attribute is per kernel, all devices alike
         if (!attr_set) {
             ck(cudaFuncSetAttribute(k_fused_tma<IDX, PML>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT_SMEM_BYTES),
                "smem attr");
             attr_set = true;
         }
-        k_fused_tma<IDX, PML><<<g, TT_THREADS, TT_SMEM_BYTES, stream>>>(tH, tE, tM, fg, ps, pn);
+        k_fused_tma<IDX, PML><<<g, TT_THREADS, TT_SMEM_BYTES, stream>>>(tH, tE, tM, fg, ps);
     }
     void launch_fused_tma(int p) {
         const FusedGrid fg = fused_grid(p);
-        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
+        const PmlSet ps = pml_set(p);
         const uint32_t bh[4] = {TT_HZ, TT_HY, 1, 3}, be[4] = {TT_EZ, TT_EY, 1, 3};
         const CUtensorMap tH = tensor_map(fg.H0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, bh);
         const CUtensorMap tE = tensor_map(fg.V0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, be);
         const CUtensorMap tM = indexed ? tensor_map(fg.mat, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, be) : tE;
         dim3 g(blocks(Nz, TT_Z), blocks(Ny, TT_Y), blocks(Nx, xchunk));
         const bool hp = !pml.empty();
-        if (indexed) { if (hp) launch_fused_tma_k<true, true>(g, tH, tE, tM, fg, ps, pn); else launch_fused_tma_k<true, false>(g, tH, tE, tM, fg, ps, pn); }
-        else { if (hp) launch_fused_tma_k<false, true>(g, tH, tE, tM, fg, ps, pn); else launch_fused_tma_k<false, false>(g, tH, tE, tM, fg, ps, pn); }
+        if (indexed) { if (hp) launch_fused_tma_k<true, true>(g, tH, tE, tM, fg, ps); else launch_fused_tma_k<true, false>(g, tH, tE, tM, fg, ps); }
+        else { if (hp) launch_fused_tma_k<false, true>(g, tH, tE, tM, fg, ps); else launch_fused_tma_k<false, false>(g, tH, tE, tM, fg, ps); }
+    }
+    // TMA path with UPML: region cells are updated by k_pml_e / k_pml_h around the fused kernel
+    bool tma_path() const { return fused && fused_kind == 2 && Nz % 4 == 0; }
+    bool pml_split() const { return tma_path() && !pml.empty(); }
+    uint32_t pml_cells() const {
+        size_t t = 0;
+        for (auto& r : pml) t += (size_t)r->n[0] * r->n[1] * r->n[2];
+        return (uint32_t)t;    // each region lies inside the grid: t <= 4N < 2^32 (at most 4 overlaps)
+    }
+    void launch_pml_e(int p) {
+        const FusedGrid fg = fused_grid(p);
+        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
+        const uint32_t t = pml_cells(), T = 256;
+        if (indexed) k_pml_e<true><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, vbuf(p), t);
+        else k_pml_e<false><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, vbuf(p), t);
+    }
+    void launch_pml_h(int p) {
+        const FusedGrid fg = fused_grid(p);
+        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
+        const uint32_t t = pml_cells(), T = 256;
+        if (indexed) k_pml_h<true><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, t);
+        else k_pml_h<false><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, t);
     }
     void launch_fused(int p) {
-        if (fused_kind == 2 && Nz % 4 == 0) {
+        if (tma_path()) {
             launch_fused_tma(p);
             return;
         }
@@ -872,6 +896,9 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
                 if (k > PML_MAX_OVERLAP) fail(EFS_ERR_RANGE, "more than 4 UPML regions overlap at one cell");
             }
         }
+        uint64_t cells = 0;   // the UPML passes of the TMA path index region cells with 32 bits
+        for (auto& R : out) cells += (uint64_t)R->n[0] * R->n[1] * R->n[2];
+        if (cells >= (1ull << 32)) fail(EFS_ERR_RANGE, "UPML regions hold 2^32 cells or more");
         e->pml = std::move(out);
         e->dirty();
     });
@@ -1436,18 +1463,25 @@ efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms) {
         for (auto& x : ev) ck(cudaEventCreate(&x), "event");
         if (e->fused) {
             // the fused kernel reads parity cur and writes the other one; repeated
-            // launches redo the same step, which is what is timed
-            ck(cudaEventRecord(ev[0], e->stream), "record");
-            for (uint32_t i = 0; i < reps; ++i) e->launch_fused(e->cur);
-            ck(cudaEventRecord(ev[1], e->stream), "record");
-            ck(cudaEventSynchronize(ev[1]), "sync");
+            // launches redo the same step, which is what is timed.  ms[0]: the fused
+            // kernel; ms[1]: the UPML passes around it (TMA path with UPML regions)
+            auto timed = [&](auto launch) {
+                ck(cudaEventRecord(ev[0], e->stream), "record");
+                for (uint32_t i = 0; i < reps; ++i) launch();
+                ck(cudaEventRecord(ev[1], e->stream), "record");
+                ck(cudaEventSynchronize(ev[1]), "sync");
+                float t = 0;
+                cudaEventElapsedTime(&t, ev[0], ev[1]);
+                return t / reps;
+            };
+            const int p = e->cur;
+            const float a = timed([&] { e->launch_fused(p); });
+            const float b = e->pml_split() ? timed([&] { e->launch_pml_e(p); }) + timed([&] { e->launch_pml_h(p); }) : 0.f;
             ck(cudaGetLastError(), "fused launch");
-            float a = 0;
-            cudaEventElapsedTime(&a, ev[0], ev[1]);
             for (auto& x : ev) cudaEventDestroy(x);
             e->sync("fused timing");
-            ms[0] = a / reps;
-            ms[1] = 0.f;
+            ms[0] = a;
+            ms[1] = b;
             return;
         }
         auto volt = [&] {
@@ -1478,7 +1512,7 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
         e->need_init();
         if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
         e->build_plan();
-        uint32_t k = e->fused ? 1 + (e->defer_n > 0) : 2;      // core: fused (+ deferred H) or E and H
+        uint32_t k = e->fused ? 1 + (e->defer_n > 0) + 2 * e->pml_split() : 2;   // fused (+ deferred H, UPML passes) or E and H
         k += e->ss_on + (e->ade_v.n > 0) + (e->ade_c.n > 0) + 3 * e->mur_on + 2 * e->rlc_on;
         k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
         k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;

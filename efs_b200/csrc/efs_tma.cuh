@@ -19,6 +19,10 @@
 // Three E_new plane buffers make step 3 of plane x and step 1 of plane x+1
 // independent, so one barrier per plane suffices.
 //
+// UPML cells are updated by k_pml_e (E, before this kernel: its E_new is
+// staged here in place of E_old and adopted as is) and k_pml_h (H, after it);
+// this kernel only needs to know which cells they are.
+//
 // Boundaries follow the reference's index-0 self reference: the x-1, y-1 and
 // z-1 neighbours of index 0 are the cell itself (the TMA zero fill outside
 // the grid is never read as a field value).  H cells whose curl reads E values
@@ -115,9 +119,11 @@ __device__ __forceinline__ void tt_issue(TmaSmem& S, int s, const CUtensorMap* t
 template <bool IDX, bool PML>
 __global__ void __launch_bounds__(TT_THREADS, 2)
 k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmE,
-            const __grid_constant__ CUtensorMap tmM, const FusedGrid g, const PmlSet ps, const PmlSet pn) {
-    extern __shared__ unsigned char smem_raw[];
-    TmaSmem& S = *reinterpret_cast<TmaSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+            const __grid_constant__ CUtensorMap tmM, const FusedGrid g, const PmlSet ps) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned working area, addressed from the shared array itself so that
+    // every access compiles to a shared-space load or store
+    TmaSmem& S = *reinterpret_cast<TmaSmem*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t z0 = blockIdx.x * TT_Z, y0 = blockIdx.y * TT_Y;
     const uint32_t xs = blockIdx.z * g.xchunk;
@@ -125,33 +131,39 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
     const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;           // last plane whose E this CTA computes
     const int nk = (int)(xl - xs) + 1;                       // planes streamed
-    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Ny = g.Ny, Nz = g.Nz;   // 3*N < 2^32
     constexpr uint64_t WAIT_NS = 1000000000ull;
+    constexpr int HPL = TT_HY * TT_HZ;                       // one component of a staged H box
+    constexpr int EPL = TT_EY * TT_EZ;                       // one component of a staged E box / E_new plane
 
     // ---- E cells of this thread: slots 0, 1 = (row, lane / lane+32); slot 2 = halo column (warp TT_Y, lanes 0..TT_Y)
-    const int row = warp;                                    // TT_Y for the halo-row warp
-    const bool has2 = (warp == TT_Y) && (lane <= TT_Y);
-    int sr[3], sc[3];
-    sr[0] = row; sc[0] = lane;
-    sr[1] = row; sc[1] = lane + 32;
-    sr[2] = has2 ? lane : 0; sc[2] = TT_Z;
     const bool own = warp < TT_Y;                            // slots 0, 1 are owned cells (E stored, H updated)
-    uint32_t sy[3], sz[3];
-    bool sin[3];
+    const bool has2 = (warp == TT_Y) && (lane <= TT_Y);
+    const int sr[3] = {warp, warp, has2 ? lane : 0};
+    const int sc[3] = {lane, lane + 32, TT_Z};
+    uint32_t sy[3], sz[3], off[3];
+    int hi[3], ei[3], dym[3], dzm[3];
+    bool sin[3], core[3];
 #pragma unroll
-    for (int s = 0; s < 3; ++s) {
-        sy[s] = y0 + sr[s]; sz[s] = z0 + sc[s];
-        sin[s] = sy[s] < g.Ny && sz[s] < g.Nz && (s < 2 || has2);
+    for (int q = 0; q < 3; ++q) {
+        sy[q] = y0 + sr[q]; sz[q] = z0 + sc[q];
+        sin[q] = sy[q] < Ny && sz[q] < Nz && (q < 2 || has2);
+        core[q] = sy[q] + 1 < Ny && sz[q] + 1 < Nz;
+        off[q] = sy[q] * Nz + sz[q];                         // offset inside a plane (used when sin)
+        hi[q] = (sr[q] + 1) * TT_HZ + sc[q] + 4;             // index in a staged H component
+        ei[q] = sr[q] * TT_EZ + sc[q];                       // index in a staged E component / E_new plane
+        dym[q] = sy[q] == 0 ? 0 : TT_HZ;                     // y-1 neighbour (self at y = 0)
+        dzm[q] = sz[q] == 0 ? 0 : 1;                         // z-1 neighbour (self at z = 0)
     }
     // UPML: regions meeting the CTA's box, then the (y, z) part of each cell's mask
     uint32_t cand = 0, yzm[3] = {0u, 0u, 0u};
     if (PML) {
         const uint32_t lo[3] = {xs, y0, z0};
-        const uint32_t hi[3] = {xe, y0 + TT_Y, z0 + TT_Z};
-        cand = region_mask(ps, lo, hi);
+        const uint32_t hb[3] = {xe, y0 + TT_Y, z0 + TT_Z};
+        cand = region_mask(ps, lo, hb);
         if (cand)
 #pragma unroll
-            for (int s = 0; s < 3; ++s) yzm[s] = axis_mask(ps, cand, 1, sy[s]) & axis_mask(ps, cand, 2, sz[s]);
+            for (int q = 0; q < 3; ++q) yzm[q] = axis_mask(ps, cand, 1, sy[q]) & axis_mask(ps, cand, 2, sz[q]);
     }
 
     // ---- pipeline set-up
@@ -169,13 +181,12 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
     // H_old(xs-1) of the E cells (y, z components); at xs = 0 the x-1 neighbour is plane 0 itself
     float hp[3][3];
     {
-        const size_t pb = (size_t)(xs > 0 ? xs - 1 : 0) * NyNz;
+        const float* H = g.H0 + (size_t)(xs > 0 ? xs - 1 : 0) * NyNz;
 #pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            hp[s][0] = 0.f;
-            const size_t c = pb + (size_t)sy[s] * Nz + sz[s];
-            hp[s][1] = sin[s] ? __ldg(g.H0 + N + c) : 0.f;
-            hp[s][2] = sin[s] ? __ldg(g.H0 + 2 * N + c) : 0.f;
+        for (int q = 0; q < 3; ++q) {
+            hp[q][0] = 0.f;
+            hp[q][1] = sin[q] ? __ldg(H + (off[q] + N)) : 0.f;
+            hp[q][2] = sin[q] ? __ldg(H + (off[q] + 2 * N)) : 0.f;
         }
     }
     float ep[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};      // E_new(x-1) of the owned cells
@@ -187,54 +198,62 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
     for (; k < nk; ++k) {
         const uint32_t x = xs + k;
         const int s = k % TT_S;
-        const TmaStage& T = S.st[s];
         const bool ok = mbar_wait_bounded(smem_u32(&S.full[s]), (uint32_t)(k / TT_S) & 1u, WAIT_NS);
         const uint32_t xmask = cand ? axis_mask(ps, cand, 0, x) : 0u;
-        float (*En)[TT_EY][TT_EZ] = S.En[k % 3];
-        const size_t px = (size_t)x * NyNz;
+        const float* Hs = &S.st[s].H[0][0][0];
+        const float* Es = &S.st[s].E[0][0][0];
+        const uint32_t* Ms = &S.st[s].M[0][0];
+        float* En = &S.En[k % 3][0][0][0];
+        const uint32_t px = x * NyNz;
         float en[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
         float hc[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        uint32_t mc[2] = {0u, 0u};
+        uint32_t mc[3] = {0u, 0u, 0u};
         if (ok) {
-            // ---- E_new(x) of the thread's cells (cells outside the grid keep E_new = 0)
+            // ---- E_new(x): gather every operand of the thread's cells, then update, then store
+            float hv[3][7], eo[3][3], kk[3][6];
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 if (q == 2 && !has2) continue;
-                const int r = sr[q], c = sc[q];
-                if (!sin[q]) {
-                    En[0][r][c] = 0.f; En[1][r][c] = 0.f; En[2][r][c] = 0.f;
-                    continue;
-                }
-                const int hr = r + 1, hcol = c + 4;                        // H box indices of the cell
-                const int hrm = sy[q] == 0 ? hr : hr - 1;                  // y-1 (self at y = 0)
-                const int hcm = sz[q] == 0 ? hcol : hcol - 1;              // z-1 (self at z = 0)
-                const float hx = T.H[0][hr][hcol], hy = T.H[1][hr][hcol], hz = T.H[2][hr][hcol];
-                const float cx = curl4(hz, T.H[2][hrm][hcol], hy, T.H[1][hr][hcm]);
-                const float cy = curl4(hx, T.H[0][hr][hcm], hz, hp[q][2]);
-                const float cz = curl4(hy, hp[q][1], hx, T.H[0][hrm][hcol]);
-                const uint32_t m = IDX ? T.M[r][c] : 0u;
-                if (q < 2) mc[q] = m;
+                const int h = hi[q], e = ei[q];
+                hv[q][0] = Hs[h]; hv[q][1] = Hs[HPL + h]; hv[q][2] = Hs[2 * HPL + h];
+                hv[q][3] = Hs[2 * HPL + h - dym[q]];         // hz(y-1)
+                hv[q][4] = Hs[HPL + h - dzm[q]];             // hy(z-1)
+                hv[q][5] = Hs[h - dzm[q]];                   // hx(z-1)
+                hv[q][6] = Hs[h - dym[q]];                   // hx(y-1)
+                eo[q][0] = Es[e]; eo[q][1] = Es[EPL + e]; eo[q][2] = Es[2 * EPL + e];
+                mc[q] = IDX ? Ms[e] : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (q == 2 && !has2) continue;
+                if (IDX) coeffs_f<true>(g, 0, mc[q], 0, kk[q]);
+                else if (sin[q]) coeffs_f<false>(g, (size_t)px + off[q], 0u, 0, kk[q]);
+                else kk[q][0] = kk[q][1] = kk[q][2] = kk[q][3] = kk[q][4] = kk[q][5] = 0.f;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (q == 2 && !has2) continue;
+                const float hx = hv[q][0], hy = hv[q][1], hz = hv[q][2];
+                const float cx = curl4(hz, hv[q][3], hy, hv[q][4]);
+                const float cy = curl4(hx, hv[q][5], hz, hp[q][2]);
+                const float cz = curl4(hy, hp[q][1], hx, hv[q][6]);
                 hc[q][0] = hx; hc[q][1] = hy; hc[q][2] = hz;
-                float kk[6];
-                coeffs_f<IDX>(g, px + (size_t)sy[q] * Nz + sz[q], m, 0, kk);
-                const float e0 = T.E[0][r][c], e1 = T.E[1][r][c], e2 = T.E[2][r][c];
-                const uint32_t cmask = PML ? (yzm[q] & xmask) : 0u;
-                if (PML && cmask) {
-                    const bool wr = own && q < 2 && x < xe;
-                    en[q][0] = pml_cell<true>(ps, pn, cmask, x, sy[q], sz[q], 0, e0, true, kk[0], kk[3], cx, wr);
-                    en[q][1] = pml_cell<true>(ps, pn, cmask, x, sy[q], sz[q], 1, e1, true, kk[1], kk[4], cy, wr);
-                    en[q][2] = pml_cell<true>(ps, pn, cmask, x, sy[q], sz[q], 2, e2, true, kk[2], kk[5], cz, wr);
-                } else {
-                    en[q][0] = upd(e0, kk[0], kk[3], cx);
-                    en[q][1] = upd(e1, kk[1], kk[4], cy);
-                    en[q][2] = upd(e2, kk[2], kk[5], cz);
-                }
-                En[0][r][c] = en[q][0]; En[1][r][c] = en[q][1]; En[2][r][c] = en[q][2];
-                if (own && q < 2 && x < xe) {
-                    const size_t cell = px + (size_t)sy[q] * Nz + sz[q];
-                    g.V1[cell] = en[q][0];
-                    g.V1[N + cell] = en[q][1];
-                    g.V1[2 * N + cell] = en[q][2];
+                // a UPML cell's E_new was computed by k_pml_e and staged in place of E_old
+                const bool upml = PML && (yzm[q] & xmask);
+                en[q][0] = upml ? eo[q][0] : upd(eo[q][0], kk[q][0], kk[q][3], cx);
+                en[q][1] = upml ? eo[q][1] : upd(eo[q][1], kk[q][1], kk[q][4], cy);
+                en[q][2] = upml ? eo[q][2] : upd(eo[q][2], kk[q][2], kk[q][5], cz);
+            }
+            float* V1 = g.V1 + px;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (q == 2 && !has2) continue;
+                const int e = ei[q];
+                En[e] = en[q][0]; En[EPL + e] = en[q][1]; En[2 * EPL + e] = en[q][2];
+                if (own && q < 2 && sin[q] && x < xe) {
+                    V1[off[q]] = en[q][0];
+                    V1[off[q] + N] = en[q][1];
+                    V1[off[q] + 2 * N] = en[q][2];
                 }
             }
         }
@@ -247,35 +266,35 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
         }
         // ---- H_new(x-1) of the owned cells
         if (k > 0 && own) {
-            const float (*Ep)[TT_EY][TT_EZ] = S.En[(k + 2) % 3];
-            const size_t pm = px - NyNz;
+            const float* Ep = &S.En[(k + 2) % 3][0][0][0];
+            float nb[2][4], kh[2][6];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                if (!sin[q]) continue;
-                const int r = sr[q], c = sc[q];
-                const bool core = (sy[q] + 1 < g.Ny) && (sz[q] + 1 < g.Nz);
-                const float ex = ep[q][0], ey = ep[q][1], ez = ep[q][2];
-                const float cx = curl4(ez, Ep[2][r + 1][c], ey, Ep[1][r][c + 1]);
-                const float cy = curl4(ex, Ep[0][r][c + 1], ez, en[q][2]);
-                const float cz = curl4(ey, en[q][1], ex, Ep[0][r + 1][c]);
-                const size_t cell = pm + (size_t)sy[q] * Nz + sz[q];
-                float kk[6];
-                coeffs_f<IDX>(g, cell, mp[q], 6, kk);
-                float hn[3];
-                const uint32_t cmask = PML ? (yzm[q] & xmask_p) : 0u;
-                if (PML && cmask) {
+                const int e = ei[q];
+                nb[q][0] = Ep[2 * EPL + e + TT_EZ];          // ez(y+1)
+                nb[q][1] = Ep[EPL + e + 1];                  // ey(z+1)
+                nb[q][2] = Ep[e + 1];                        // ex(z+1)
+                nb[q][3] = Ep[e + TT_EZ];                    // ex(y+1)
+                if (IDX) coeffs_f<true>(g, 0, mp[q], 6, kh[q]);
+                else if (sin[q]) coeffs_f<false>(g, (size_t)(px - NyNz) + off[q], 0u, 6, kh[q]);
+                else kh[q][0] = kh[q][1] = kh[q][2] = kh[q][3] = kh[q][4] = kh[q][5] = 0.f;
+            }
+            float* H1 = g.H1 + (px - NyNz);
 #pragma unroll
-                    for (int n = 0; n < 3; ++n)
-                        hn[n] = pml_cell<false>(ps, pn, cmask, x - 1, sy[q], sz[q], n, hp[q][n], core, kk[n], kk[3 + n],
-                                                n == 0 ? cx : (n == 1 ? cy : cz), true);
-                } else {
-                    hn[0] = core ? upd(hp[q][0], kk[0], kk[3], cx) : hp[q][0];
-                    hn[1] = core ? upd(hp[q][1], kk[1], kk[4], cy) : hp[q][1];
-                    hn[2] = core ? upd(hp[q][2], kk[2], kk[5], cz) : hp[q][2];
+            for (int q = 0; q < 2; ++q) {
+                const float ex = ep[q][0], ey = ep[q][1], ez = ep[q][2];
+                const float cx = curl4(ez, nb[q][0], ey, nb[q][1]);
+                const float cy = curl4(ex, nb[q][2], ez, en[q][2]);
+                const float cz = curl4(ey, en[q][1], ex, nb[q][3]);
+                float hn[3];
+                hn[0] = core[q] ? upd(hp[q][0], kh[q][0], kh[q][3], cx) : hp[q][0];
+                hn[1] = core[q] ? upd(hp[q][1], kh[q][1], kh[q][4], cy) : hp[q][1];
+                hn[2] = core[q] ? upd(hp[q][2], kh[q][2], kh[q][5], cz) : hp[q][2];
+                if (sin[q] && !(PML && (yzm[q] & xmask_p))) {     // UPML cells: k_pml_h
+                    H1[off[q]] = hn[0];
+                    H1[off[q] + N] = hn[1];
+                    H1[off[q] + 2 * N] = hn[2];
                 }
-                g.H1[cell] = hn[0];
-                g.H1[N + cell] = hn[1];
-                g.H1[2 * N + cell] = hn[2];
             }
         }
         // ---- rotate
@@ -294,21 +313,101 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
         }
         return;
     }
-    // ---- H of the last plane x = Nx-1: no core update, UPML / pass-through only
+    // ---- H of the last plane x = Nx-1: no core update (pass-through; UPML cells: k_pml_h)
     if (xe == g.Nx && own) {
-        const size_t pl = (size_t)(g.Nx - 1) * NyNz;
+        float* H1 = g.H1 + (size_t)(g.Nx - 1) * NyNz;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            if (!sin[q]) continue;
-            const size_t cell = pl + (size_t)sy[q] * Nz + sz[q];
-            const uint32_t cmask = PML ? (yzm[q] & xmask_p) : 0u;
+            if (!sin[q] || (PML && (yzm[q] & xmask_p))) continue;
 #pragma unroll
-            for (int n = 0; n < 3; ++n)
-                g.H1[n * N + cell] = (PML && cmask)
-                    ? pml_cell<false>(ps, pn, cmask, g.Nx - 1, sy[q], sz[q], n, hp[q][n], false, 0.f, 0.f, 0.f, true)
-                    : hp[q][n];
+            for (int n = 0; n < 3; ++n) H1[off[q] + n * N] = hp[q][n];
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// UPML cells of the TMA path, outside the streaming kernel.  Their update
+// reads per-cell region coefficients and fluxes with dependent loads; run
+// inside the plane pipeline those loads stalled every CTA whose tile touches a
+// region.  k_pml_e runs before k_fused_tma and k_pml_h after it, one thread
+// per UPML cell (z fastest within a region, so accesses coalesce).  A cell
+// that several regions contain is handled once, by the first of them, with
+// the chain over all of them in region order.
+// ---------------------------------------------------------------------------
+
+// Cell of flat index i over the regions' boxes; false when a lower-numbered
+// region also contains it.  `mask`: every region containing the cell.
+__device__ __forceinline__ bool pml_locate(const PmlSet& ps, uint32_t i, uint32_t& x, uint32_t& y, uint32_t& z,
+                                           uint32_t& mask) {
+    int r = 0;
+    for (; r < ps.count; ++r) {
+        const uint32_t c = ps.r[r].n[0] * ps.r[r].n[1] * ps.r[r].n[2];
+        if (i < c) break;
+        i -= c;
+    }
+    if (r == ps.count) return false;
+    const PmlRegion& R = ps.r[r];
+    const uint32_t nyz = R.n[1] * R.n[2];
+    x = R.s[0] + i / nyz;
+    y = R.s[1] + (i % nyz) / R.n[2];
+    z = R.s[2] + i % R.n[2];
+    for (int q = 0; q < r; ++q)
+        if (in_region(ps.r[q], x, y, z)) return false;
+    mask = 0;
+    for (int q = r; q < ps.count; ++q)
+        if (in_region(ps.r[q], x, y, z)) mask |= 1u << q;
+    return true;
+}
+
+// E_new of the UPML cells (reads H_old and E_old, the old flux; writes the new
+// flux).  E_new is written over E_old in `V0w` (the step's old-E buffer, dead
+// after this step's core update), where k_fused_tma stages it.
+template <bool IDX>
+__global__ void k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    uint32_t x, y, z, mask;
+    if (!pml_locate(ps, i, x, y, z, mask)) return;
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;
+    const uint32_t c = x * NyNz + y * Nz + z;
+    const uint32_t xm = x > 0 ? c - NyNz : c, ym = y > 0 ? c - Nz : c, zm = z > 0 ? c - 1 : c;   // self at index 0
+    const float* H = g.H0;
+    const float cx = curl4(H[2 * N + c], H[2 * N + ym], H[N + c], H[N + zm]);
+    const float cy = curl4(H[c], H[zm], H[2 * N + c], H[2 * N + xm]);
+    const float cz = curl4(H[N + c], H[N + xm], H[c], H[ym]);
+    float kk[6];
+    coeffs_f<IDX>(g, c, IDX ? __ldg(g.mat + c) : 0u, 0, kk);
+    const float e0 = V0w[c], e1 = V0w[N + c], e2 = V0w[2 * N + c];
+    const float n0 = pml_chain_pp<true>(ps, pn, mask, x, y, z, 0, e0, true, kk[0], kk[3], cx, true);
+    const float n1 = pml_chain_pp<true>(ps, pn, mask, x, y, z, 1, e1, true, kk[1], kk[4], cy, true);
+    const float n2 = pml_chain_pp<true>(ps, pn, mask, x, y, z, 2, e2, true, kk[2], kk[5], cz, true);
+    V0w[c] = n0; V0w[N + c] = n1; V0w[2 * N + c] = n2;
+}
+
+// H_new of the UPML cells from the final-core E_new (cells whose curl reads E
+// rewritten by a sparse operation are redone by k_deferred_h).
+template <bool IDX>
+__global__ void k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    uint32_t x, y, z, mask;
+    if (!pml_locate(ps, i, x, y, z, mask)) return;
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;
+    const uint32_t c = x * NyNz + y * Nz + z;
+    const bool core = (x + 1 < g.Nx) && (y + 1 < g.Ny) && (z + 1 < g.Nz);
+    const float* V = g.V1;
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (core) {
+        cx = curl4(V[2 * N + c], V[2 * N + c + Nz], V[N + c], V[N + c + 1]);
+        cy = curl4(V[c], V[c + 1], V[2 * N + c], V[2 * N + c + NyNz]);
+        cz = curl4(V[N + c], V[N + c + NyNz], V[c], V[c + Nz]);
+        coeffs_f<IDX>(g, c, IDX ? __ldg(g.mat + c) : 0u, 6, kk);
+    }
+    const float h0 = pml_chain_pp<false>(ps, pn, mask, x, y, z, 0, g.H0[c], core, kk[0], kk[3], cx, true);
+    const float h1 = pml_chain_pp<false>(ps, pn, mask, x, y, z, 1, g.H0[N + c], core, kk[1], kk[4], cy, true);
+    const float h2 = pml_chain_pp<false>(ps, pn, mask, x, y, z, 2, g.H0[2 * N + c], core, kk[2], kk[5], cz, true);
+    g.H1[c] = h0; g.H1[N + c] = h1; g.H1[2 * N + c] = h2;
 }
 
 }  // namespace efs

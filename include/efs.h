@@ -251,9 +251,10 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
 
 /* Diagnostics: launch the engine's core field-update kernel(s) `reps` times
  * on its stream and return the mean device time per launch (CUDA events).
- * ms[0] = E update, ms[1] = H update (ms[1] = 0 when one fused kernel
- * updates both).  Advances the fields; meant for benchmarks only.  No
- * counterpart in the reference. */
+ * Separate sweeps: ms[0] = E update, ms[1] = H update.  Fused path: ms[0] =
+ * the fused E+H kernel, ms[1] = the UPML-cell passes around it (0 without
+ * UPML regions or off the TMA-fed kernel).  Advances the fields; meant for
+ * benchmarks only.  No counterpart in the reference. */
 efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms);
 
 /* Diagnostics: kernel launches one timestep enqueues with the current
