@@ -162,8 +162,8 @@ def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_ins
 def job_bytes_per_step(job):
     """Algorithmic HBM bytes of one timestep of `job` (fields read+written once,
     one u32 material index per cell, UPML/Mur/TFSF/NF2FF/probe traffic):
-    core 48 B + 4 B per cell; UPML 24 B flux r/w + 72 B coefficients per
-    region cell (3 components); Mur 3 passes ~ 28 B per point; TFSF/excitation
+    core 48 B + 4 B per cell; UPML 48 B flux r/w (E and H) + 72 B coefficients
+    per region cell (3 components); Mur 3 passes ~ 28 B per point; TFSF/excitation
     16 B per point; NF2FF 24 B field reads + 96 B accumulator r/w per
     point-frequency."""
     Nx, Ny, Nz = job["grid"]
@@ -172,7 +172,7 @@ def job_bytes_per_step(job):
     b = N * (48 + coeff)
     for r in job.get("pml") or []:
         c = r["numLines"][0] * r["numLines"][1] * r["numLines"][2]
-        b += c * (24 + 72)
+        b += c * (48 + 72)
     if job.get("mur"):
         b += 28 * (len(job["mur"]["coeff_nyP"]) + len(job["mur"]["coeff_nyPP"]))
     if job.get("tfsf"):
