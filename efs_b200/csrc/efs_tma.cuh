@@ -120,10 +120,10 @@ template <bool IDX, bool PML>
 __global__ void __launch_bounds__(TT_THREADS, 2)
 k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmE,
             const __grid_constant__ CUtensorMap tmM, const FusedGrid g, const PmlSet ps) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char tt_smem_raw[];
     // 128-byte aligned working area, addressed from the shared array itself so that
     // every access compiles to a shared-space load or store
-    TmaSmem& S = *reinterpret_cast<TmaSmem*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
+    TmaSmem& S = *reinterpret_cast<TmaSmem*>(tt_smem_raw + ((128u - (smem_u32(tt_smem_raw) & 127u)) & 127u));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t z0 = blockIdx.x * TT_Z, y0 = blockIdx.y * TT_Y;
     const uint32_t xs = blockIdx.z * g.xchunk;
