@@ -73,6 +73,7 @@ SIGNATURES = {
     "efs_far_field": (C.c_int, [vp, u32, f32p, f32p, u32, f32p, u32, f64p, C.c_double, C.c_double, f32p]),
     "efs_energy": (C.c_int, [vp, C.c_int, f64p]),
     "efs_flush_energy": (C.c_int, [vp, f64p]),
+    "efs_energy_noalloc": (C.c_int, [vp, f64p]),
     "efs_get_fields": (C.c_int, [vp, f32p, f32p]),
     "efs_set_fields": (C.c_int, [vp, f32p, f32p]),
     "efs_get_state": (C.c_int, [vp, vp, szt, C.POINTER(szt)]),

@@ -32,6 +32,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -1312,6 +1313,59 @@ efs_status efs_energy(efs_engine* e, int lagged, double* out) {
         e->en_pending = true;
         e->en_idx = prev;
         *out = e->en_last;
+    });
+}
+
+// ---- energy without device allocation ---------------------------------------
+// Scratch of efs_energy_noalloc: a fixed array inside this library (every GPU
+// that loads it holds one copy until exit).  Slots [0, EN_NA_MAX_PARTIALS)
+// take one partial sum per EN_NA_CELLS interior cells, the last slot the
+// result.  A call writes every slot it reads before reading it, so nothing
+// carries over from the previous call and nothing needs clearing.  All calls
+// on a device share it: calls that overlap on the GPU race.
+constexpr uint64_t EN_NA_CELLS = 65536;            // interior cells per partial sum
+constexpr uint32_t EN_NA_MAX_PARTIALS = 16384;     // => at most 2^30 interior cells
+constexpr int EN_NA_MAX_DEVICES = 64;
+static __device__ __align__(256) double g_energy_noalloc[EN_NA_MAX_PARTIALS + 1];
+static double* g_energy_noalloc_addr[EN_NA_MAX_DEVICES];   // device address per device ordinal
+static std::mutex g_energy_noalloc_mu;
+
+// Device address of g_energy_noalloc on `device`, which the caller has made
+// current.  Host code cannot use the array's name as a device pointer: the
+// first call per device asks the runtime for the address once.
+static double* energy_noalloc_scratch(int device) {
+    if (device < 0 || device >= EN_NA_MAX_DEVICES) fail(EFS_ERR_RANGE, "efs_energy_noalloc: device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_energy_noalloc_mu);
+    if (!g_energy_noalloc_addr[device]) {
+        void* p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_energy_noalloc), "efs_energy_noalloc: cudaGetSymbolAddress");
+        if (!p) fail(EFS_ERR_CUDA, "efs_energy_noalloc: no device address for the scratch array");
+        g_energy_noalloc_addr[device] = static_cast<double*>(p);
+    }
+    return g_energy_noalloc_addr[device];
+}
+
+efs_status efs_energy_noalloc(efs_engine* e, double* out) {
+    return guard(e, [&] {
+        e->need_init();
+        if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
+        const uint64_t inner = (e->Nx < 2 || e->Ny < 2 || e->Nz < 2)
+                                   ? 0 : (uint64_t)(e->Nx - 1) * (e->Ny - 1) * (e->Nz - 1);
+        const uint64_t parts = (inner + EN_NA_CELLS - 1) / EN_NA_CELLS;
+        if (parts > EN_NA_MAX_PARTIALS)
+            fail(EFS_ERR_RANGE, "efs_energy_noalloc: the grid has " + std::to_string(inner) +
+                                    " interior cells; its fixed scratch covers at most 2^30 (16384 partial sums of 65536 cells)");
+        double* scratch = energy_noalloc_scratch(e->device);
+        if (parts == 0) {
+            *out = 0.0;
+            return;
+        }
+        double* result = scratch + EN_NA_MAX_PARTIALS;
+        k_energy_ranges<<<(uint32_t)parts, 256, 0, e->stream>>>(e->vcur(), e->ccur(), e->Nx, e->Ny, e->Nz, EN_NA_CELLS, scratch);
+        k_energy_final<<<1, 1024, 0, e->stream>>>(scratch, (uint32_t)parts, result);
+        ck(cudaGetLastError(), "efs_energy_noalloc");
+        ck(cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "efs_energy_noalloc readback");
+        e->sync("efs_energy_noalloc");
     });
 }
 

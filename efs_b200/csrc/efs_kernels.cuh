@@ -607,6 +607,38 @@ __global__ void k_energy_final(const double* partial, uint32_t n, double* out) {
     }
 }
 
+// Variant of k_energy for the allocation-free entry point: block b sums the
+// interior cells [b*cells, (b+1)*cells) (interior index order) into
+// partial[b], so the number of partial sums grows with the grid and a fixed
+// scratch array bounds the grid it accepts.  Same per-cell f32 arithmetic.
+__global__ void __launch_bounds__(256) k_energy_ranges(const float* __restrict__ V, const float* __restrict__ C, uint32_t Nx,
+                                                       uint32_t Ny, uint32_t Nz, uint64_t cells, double* partial) {
+    const size_t N = (size_t)Nx * Ny * Nz, inner = (size_t)(Nx - 1) * (Ny - 1) * (Nz - 1);
+    const size_t iNz = Nz - 1, iNyNz = (size_t)(Ny - 1) * (Nz - 1);
+    const size_t lo = (size_t)blockIdx.x * cells, hi = min(lo + cells, inner);
+    double acc = 0.0;
+    for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const size_t x = i / iNyNz, r = i - x * iNyNz, y = r / iNz, z = r - y * iNz;
+        const size_t c = x * Ny * Nz + y * Nz + z;
+        float s = 0.f;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            const float v = __ldg(V + n * N + c), h = __ldg(C + n * N + c);
+            s = __fadd_rn(__fadd_rn(s, __fmul_rn(v, v)), __fmul_rn(h, h));
+        }
+        acc += (double)s;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // NF2FF far field (src/webgpu-engine.mjs:830-985).  Thread = one (theta,phi)
 // angle; a block stages a tile of surface points in shared memory (surface

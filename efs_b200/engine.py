@@ -392,6 +392,14 @@ class CudaEngine:
         self._ck(self._lib.efs_flush_energy(self._h, C.byref(v)))
         return v.value
 
+    def energyNoAlloc(self):
+        """Current energy (as computeEnergy(lagged=False)) with no device
+        allocation: for callers that keep the library from allocating once
+        they run (efs_energy_noalloc)."""
+        v = C.c_double()
+        self._ck(self._lib.efs_energy_noalloc(self._h, C.byref(v)))
+        return v.value
+
     # --- state --------------------------------------------------------
     def getFields(self):
         n = 3 * self.totalCells

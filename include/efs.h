@@ -222,6 +222,22 @@ efs_status efs_far_field(efs_engine* e, uint32_t freq_index, const float* point_
 efs_status efs_energy(efs_engine* e, int lagged, double* out);
 /* flushEnergy (:3027-3037). */
 efs_status efs_flush_energy(efs_engine* e, double* out);
+/* The current energy (what efs_energy returns with lagged == 0), computed
+ * without allocating any device memory.  For callers that cannot let the
+ * library call cudaMalloc once they are running: a server that reserves its
+ * whole HBM budget for solves up front, or a host runtime that owns every
+ * device allocation, where a lazy allocation could fail mid-run or break the
+ * caller's accounting (efs_energy allocates its scratch on first use).
+ * Scratch is a fixed array inside libefs.so: 16384 partial sums + 1 result
+ * (128 KB), held by every GPU that loads the library until the process
+ * exits; a grid with more than 2^30 interior cells returns EFS_ERR_RANGE.
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture.  All calls on a device share
+ * the array (each call writes what it reads, so nothing needs clearing):
+ * calls that overlap on the GPU, e.g. two engines on one device driven from
+ * two threads, race.  Sums in a different order than efs_energy (agrees to
+ * ~1e-12 relative).  No counterpart in the reference. */
+efs_status efs_energy_noalloc(efs_engine* e, double* out);
 
 /* --- state transfer ---------------------------------------------------- */
 
