@@ -263,9 +263,12 @@ def run_b200(args):
             "ms_per_launch": round(core_ms[0], 4), "upml_passes_ms": round(core_ms[1], 4),
             "peak_kind": "of " + peak_kind}
     step_bytes = workloads.job_bytes_per_step(job)
-    # our kernels in the timed region: per timestep plan + one counter update per
-    # captured graph (64 steps each) + the two energy-reduction kernels per step
-    launches = args.steps * (BATCH * eng.kernelsPerStep() + math.ceil(BATCH / 64) + 2)
+    # our kernels in the timed region: per timestep plan + per captured graph (64
+    # steps each) one counter update and ceil(m/16) NF2FF accumulator passes +
+    # the two energy-reduction kernels per step
+    chunks = [64] * (BATCH // 64) + ([BATCH % 64] if BATCH % 64 else [])
+    nf_passes = sum(math.ceil(m / 16) for m in chunks) if job.get("nf2ff") else 0
+    launches = args.steps * (BATCH * eng.kernelsPerStep() + len(chunks) + nf_passes + 2)
     eng.destroy()
 
     # end to end through the public API from host buffers

@@ -178,7 +178,7 @@ struct efs_engine {
 
     // NF2FF
     bool nf_on = false;
-    DevBuf nf_pts, nf_el, nf_E, nf_H;
+    DevBuf nf_pts, nf_el, nf_E, nf_H, nf_samp;
     Nf2ffDev nf{};
 
     // energy (lagged, double-buffered like computeEnergy :2974-3021)
@@ -388,7 +388,8 @@ struct efs_engine {
 
     // Enqueue timestep k of a batch (numTS = state.numTS + k); the fields are
     // read from parity p and, on the fused path, written to parity 1 - p.
-    void enqueue_step(uint32_t k, int p) {
+    // `last`: k is the batch's final step (buffered NF2FF samples are flushed).
+    void enqueue_step(uint32_t k, int p, bool last) {
         const int q = pnext(p);
         const Grid g = grid(p);
         const PmlSet ps = pml_set(p);
@@ -454,7 +455,13 @@ struct efs_engine {
         if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C1, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
         if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, false, C1);
         // --- after the step ---
-        if (nf_on) k_nf2ff<<<blocks(nf.np, T), T, 0, stream>>>(V1, C1, st, k, nf);
+        if (nf_on) {
+            // surface samples of this step; the accumulators take every NF_K steps
+            // and the batch's last step (nothing stays pending between batches)
+            const uint32_t j = k % NF_K;
+            k_nf2ff_sample<<<blocks(nf.np, T), T, 0, stream>>>(V1, C1, j, nf);
+            if (j == NF_K - 1 || last) k_nf2ff_flush<<<blocks(nf.np, T), T, 0, stream>>>(st, k - j, j + 1, nf);
+        }
         if (ring_on)
             k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V1, C1, st, k, ring_idx.as<uint32_t>(), ring_n, ring_interval,
                                                                   ring_q0, ring_max, ring.as<float>());
@@ -539,22 +546,22 @@ struct efs_engine {
     // TMA path with UPML: region cells are updated by k_pml_e / k_pml_h around the fused kernel
     bool tma_path() const { return fused && fused_kind == 2 && Nz % 4 == 0; }
     bool pml_split() const { return tma_path() && !pml.empty(); }
-    uint32_t pml_cells() const {
+    uint32_t pml_items() const {   // work items of k_pml_e / k_pml_h: PML_ZC cells of a region row each
         size_t t = 0;
-        for (auto& r : pml) t += (size_t)r->n[0] * r->n[1] * r->n[2];
-        return (uint32_t)t;    // each region lies inside the grid: t <= 4N < 2^32 (at most 4 overlaps)
+        for (auto& r : pml) t += (size_t)r->n[0] * r->n[1] * ((r->n[2] + PML_ZC - 1) / PML_ZC);
+        return (uint32_t)t;    // at most the regions' cell count, < 2^32 (efs_configure_pml)
     }
     void launch_pml_e(int p) {
         const FusedGrid fg = fused_grid(p);
         const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
-        const uint32_t t = pml_cells(), T = 256;
+        const uint32_t t = pml_items(), T = 256;
         if (indexed) k_pml_e<true><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, vbuf(p), t);
         else k_pml_e<false><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, vbuf(p), t);
     }
     void launch_pml_h(int p) {
         const FusedGrid fg = fused_grid(p);
         const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
-        const uint32_t t = pml_cells(), T = 256;
+        const uint32_t t = pml_items(), T = 256;
         if (indexed) k_pml_h<true><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, t);
         else k_pml_h<false><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, t);
     }
@@ -629,7 +636,7 @@ struct efs_engine {
         ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "BeginCapture");
         try {
             int q = p;
-            for (uint32_t k = 0; k < m; ++k) { enqueue_step(k, q); q = pnext(q); }
+            for (uint32_t k = 0; k < m; ++k) { enqueue_step(k, q, k + 1 == m); q = pnext(q); }
             k_advance<<<1, 1, 0, stream>>>(state.as<StepState>(), m);
         } catch (...) {
             cudaStreamEndCapture(stream, &graph);
@@ -1200,6 +1207,7 @@ efs_status efs_configure_nf2ff(efs_engine* e, const uint32_t* pts, uint32_t np, 
         e->upload(e->nf_el, el, nel);
         e->alloc(e->nf_E, (size_t)nf * np * 6 * 4);
         e->alloc(e->nf_H, (size_t)nf * np * 6 * 4);
+        e->alloc(e->nf_samp, (size_t)NF_K * 6 * np * 4, false);   // written before read each pass
         Nf2ffDev& d = e->nf;
         memset(&d, 0, sizeof(d));
         d.np = np; d.nf = nf; d.maxTS = maxTS; d.window = window;
@@ -1209,6 +1217,7 @@ efs_status efs_configure_nf2ff(efs_engine* e, const uint32_t* pts, uint32_t np, 
         for (int k = 0; k < 6; ++k) { d.off[k] = o; o += nl[k % 3]; }
         d.pts = e->nf_pts.as<uint32_t>(); d.el = e->nf_el.as<float>();
         d.accE = e->nf_E.as<float>(); d.accH = e->nf_H.as<float>();
+        d.samp = e->nf_samp.as<float>();
         for (uint32_t f = 0; f < nf; ++f) d.wdt[f] = omegas[f] * dT;
         d.dT32 = (float)dT;
         double wn = 1.0;
@@ -1584,7 +1593,7 @@ efs_status efs_device_bytes(const efs_engine* e, size_t* out) {
         const DevBuf* rb[] = {&r->vv, &r->vvfo, &r->vvfn, &r->ii, &r->iifo, &r->iifn, &r->vflux, &r->cflux, &r->vflux_b, &r->cflux_b};
         for (auto* b : rb) t += b->bytes;
     }
-    t += e->nf_E.bytes + e->nf_H.bytes + e->ring.bytes;
+    t += e->nf_E.bytes + e->nf_H.bytes + e->nf_samp.bytes + e->ring.bytes;
     *out = t;
     return EFS_OK;
 }

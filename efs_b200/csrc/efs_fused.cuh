@@ -653,28 +653,38 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
 // H update of the deferred cells, after the E-side sparse operations:
 // reads the final E_new, H_old, writes H_new (with UPML), one thread per cell.
 template <bool IDX, bool PML>
-__global__ void k_deferred_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, const uint32_t* cells, uint32_t n) {
+__global__ void __launch_bounds__(256) k_deferred_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, const uint32_t* cells,
+                                                    uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const size_t c = cells[i];
-    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
-    const uint32_t x = (uint32_t)(c / NyNz), y = (uint32_t)((c / Nz) % g.Ny), z = (uint32_t)(c % Nz);
+    const uint32_t c = cells[i];
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;   // 3*N < 2^32
+    const uint32_t x = c / NyNz, rem = c - x * NyNz, y = rem / Nz, z = rem - y * Nz;
     const bool core = (x + 1 < g.Nx) && (y + 1 < g.Ny) && (z + 1 < g.Nz);
     const float* V = g.V1;
-    float cx = 0.f, cy = 0.f, cz = 0.f;
+    float ho[3], ev[9];
+    ho[0] = g.H0[c]; ho[1] = g.H0[N + c]; ho[2] = g.H0[2 * N + c];
+    uint32_t m = 0;
+    if (core) {
+        ev[0] = V[c]; ev[1] = V[N + c]; ev[2] = V[2 * N + c];
+        ev[3] = V[2 * N + c + Nz]; ev[4] = V[N + c + 1]; ev[5] = V[c + 1];
+        ev[6] = V[2 * N + c + NyNz]; ev[7] = V[N + c + NyNz]; ev[8] = V[c + Nz];
+        m = IDX ? __ldg(g.mat + c) : 0u;
+    }
+    float cv[3] = {0.f, 0.f, 0.f};
     float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (core) {
-        cx = curl4(V[2 * N + c], V[2 * N + c + Nz], V[N + c], V[N + c + 1]);
-        cy = curl4(V[c], V[c + 1], V[2 * N + c], V[2 * N + c + NyNz]);
-        cz = curl4(V[N + c], V[N + c + NyNz], V[c], V[c + Nz]);
-        coeffs_f<IDX>(g, c, IDX ? __ldg(g.mat + c) : 0u, 6, kk);
+        cv[0] = curl4(ev[2], ev[3], ev[1], ev[4]);
+        cv[1] = curl4(ev[0], ev[5], ev[2], ev[6]);
+        cv[2] = curl4(ev[1], ev[7], ev[0], ev[8]);
+        coeffs_f<IDX>(g, c, m, 6, kk);
     }
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-        const float ho = g.H0[q * N + c];
         float hn;
-        if (PML) hn = pml_chain_pp<false>(ps, pn, ps.count >= 32 ? ~0u : ((1u << ps.count) - 1u), x, y, z, q, ho, core, kk[q], kk[3 + q], q == 0 ? cx : (q == 1 ? cy : cz), true);
-        else hn = core ? upd(ho, kk[q], kk[3 + q], q == 0 ? cx : (q == 1 ? cy : cz)) : ho;
+        if (PML) hn = pml_chain_pp<false>(ps, pn, ps.count >= 32 ? ~0u : ((1u << ps.count) - 1u), x, y, z, q, ho[q], core,
+                                          kk[q], kk[3 + q], cv[q], true);
+        else hn = core ? upd(ho[q], kk[q], kk[3 + q], cv[q]) : ho[q];
         g.H1[q * N + c] = hn;
     }
 }

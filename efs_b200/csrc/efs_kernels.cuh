@@ -483,6 +483,7 @@ __global__ void k_advance(StepState* st, uint32_t n) { st->numTS += n; }
 // as n grows); the accumulation stays f32 in the reference's operand order.
 // ---------------------------------------------------------------------------
 constexpr int NF_MAX_FREQ = 16;
+constexpr uint32_t NF_K = 16;       // steps of surface samples buffered between accumulator passes
 struct Nf2ffDev {
     uint32_t np, nf, maxTS, window;
     uint32_t Nx, Ny, Nz;
@@ -490,41 +491,20 @@ struct Nf2ffDev {
     const uint32_t* pts;
     const float* el;
     float* accE; float* accH;       // [f][pid*6+k]
+    float* samp;                    // [NF_K][6][np]: buffered E, H samples
     double wdt[NF_MAX_FREQ];        // omega*dT per frequency (f64)
     float dT32, wnorm;
 };
-__global__ void __launch_bounds__(256) k_nf2ff(const float* __restrict__ V, const float* __restrict__ C, const StepState* st,
-                                               uint32_t k, const Nf2ffDev d) {
-    __shared__ float tw[NF_MAX_FREQ][4];
-    __shared__ float s_wdt;
-    const uint32_t ts = st->numTS + k + 1;     // WebGPUEngine.iterate passes numTS+1 (:2484)
-    if (threadIdx.x < d.nf) {
-        const double two_pi = 6.283185307179586476925286766559;
-        const double pe = fmod(d.wdt[threadIdx.x] * (double)ts, two_pi);
-        const double ph = fmod(d.wdt[threadIdx.x] * ((double)ts + 0.5), two_pi);
-        double s, c;
-        sincos(pe, &s, &c);
-        tw[threadIdx.x][0] = (float)c; tw[threadIdx.x][1] = (float)s;
-        sincos(ph, &s, &c);
-        tw[threadIdx.x][2] = (float)c; tw[threadIdx.x][3] = (float)s;
-    }
-    if (threadIdx.x == 0) {
-        float ww = 1.0f;
-        if (d.window == 1 && d.maxTS > 1) {
-            const double two_pi = 6.283185307179586476925286766559;
-            ww = (float)(0.5 * (1.0 - cos(two_pi * (double)ts / (double)(d.maxTS - 1))));
-        }
-        s_wdt = __fmul_rn(__fmul_rn(ww, d.wnorm), d.dT32);
-    }
-    __syncthreads();
-    const uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pid >= d.np) return;
+// Cell-interpolated E and H at surface point pid (webgpu-engine.mjs:690-761).
+__device__ __forceinline__ void nf2ff_fields(const float* __restrict__ V, const float* __restrict__ C, const Nf2ffDev& d,
+                                             uint32_t pid, float E[3], float Hh[3]) {
     const uint32_t ix = d.pts[3 * pid], iy = d.pts[3 * pid + 1], iz = d.pts[3 * pid + 2];
     const size_t Ny = d.Ny, Nz = d.Nz, N = (size_t)d.Nx * Ny * Nz, NyNz = Ny * Nz;
     auto fi = [&](uint32_t x, uint32_t y, uint32_t z) { return (size_t)x * NyNz + (size_t)y * Nz + z; };
     const size_t base = fi(ix, iy, iz);
     const bool atB = (ix >= d.Nx - 1) || (iy >= d.Ny - 1) || (iz >= d.Nz - 1);
-    float E[3] = {0.f, 0.f, 0.f}, Hh[3] = {0.f, 0.f, 0.f};
+    E[0] = E[1] = E[2] = 0.f;
+    Hh[0] = Hh[1] = Hh[2] = 0.f;
     if (!atB) {
         const float elX = d.el[d.off[0] + ix], elY = d.el[d.off[1] + iy], elZ = d.el[d.off[2] + iz];
         float a = __fadd_rn(__fadd_rn(__fadd_rn(V[base], V[fi(ix, iy + 1, iz)]), V[fi(ix, iy + 1, iz + 1)]), V[fi(ix, iy, iz + 1)]);
@@ -548,17 +528,90 @@ __global__ void __launch_bounds__(256) k_nf2ff(const float* __restrict__ V, cons
         }
         Hh[n] = h;
     }
-    const float w = s_wdt;
-    for (uint32_t f = 0; f < d.nf; ++f) {
-        float* aE = d.accE + ((size_t)f * d.np + pid) * 6;
-        float* aH = d.accH + ((size_t)f * d.np + pid) * 6;
-        const float ce = tw[f][0], se = -tw[f][1], ch = tw[f][2], sh = -tw[f][3];
+}
+
+// Every step: the interpolated surface fields of the step into sample slot
+// `slot` ([slot][6][np], E then H components).
+__global__ void __launch_bounds__(256) k_nf2ff_sample(const float* __restrict__ V, const float* __restrict__ C, uint32_t slot,
+                                                      const Nf2ffDev d) {
+    const uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= d.np) return;
+    float E[3], Hh[3];
+    nf2ff_fields(V, C, d, pid, E, Hh);
+    float* s = d.samp + (size_t)slot * 6 * d.np + pid;
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            aE[2 * n] = __fadd_rn(aE[2 * n], __fmul_rn(__fmul_rn(E[n], ce), w));
-            aE[2 * n + 1] = __fadd_rn(aE[2 * n + 1], __fmul_rn(__fmul_rn(E[n], se), w));
-            aH[2 * n] = __fadd_rn(aH[2 * n], __fmul_rn(__fmul_rn(Hh[n], ch), w));
-            aH[2 * n + 1] = __fadd_rn(aH[2 * n + 1], __fmul_rn(__fmul_rn(Hh[n], sh), w));
+    for (int n = 0; n < 3; ++n) {
+        s[(size_t)n * d.np] = E[n];
+        s[(size_t)(3 + n) * d.np] = Hh[n];
+    }
+}
+
+// Running DFT of `cnt` buffered steps (timesteps numTS+k0+1 .. numTS+k0+cnt,
+// WebGPUEngine.iterate passes numTS+1, :2484): each accumulator is loaded
+// once, takes the steps' terms in step order (the same operations, in the
+// same order, as one accumulation per step) and is stored once.  Phase per
+// step and frequency in f64 reduced mod 2*pi, then rounded to f32.
+constexpr int NF_FG = 4;   // frequencies per register group
+__global__ void __launch_bounds__(256) k_nf2ff_flush(const StepState* st, uint32_t k0, uint32_t cnt, const Nf2ffDev d) {
+    __shared__ float tw[NF_K][NF_MAX_FREQ][4];
+    __shared__ float sw[NF_K];
+    const uint32_t ts0 = st->numTS + k0 + 1;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (uint32_t i = threadIdx.x; i < cnt * d.nf; i += blockDim.x) {
+        const uint32_t j = i / d.nf, f = i - j * d.nf;
+        const double ts = (double)(ts0 + j);
+        const double pe = fmod(d.wdt[f] * ts, two_pi);
+        const double ph = fmod(d.wdt[f] * (ts + 0.5), two_pi);
+        double sn, cs;
+        sincos(pe, &sn, &cs);
+        tw[j][f][0] = (float)cs; tw[j][f][1] = (float)sn;
+        sincos(ph, &sn, &cs);
+        tw[j][f][2] = (float)cs; tw[j][f][3] = (float)sn;
+    }
+    for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+        float ww = 1.0f;
+        if (d.window == 1 && d.maxTS > 1) ww = (float)(0.5 * (1.0 - cos(two_pi * (double)(ts0 + j) / (double)(d.maxTS - 1))));
+        sw[j] = __fmul_rn(__fmul_rn(ww, d.wnorm), d.dT32);
+    }
+    __syncthreads();
+    const uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= d.np) return;
+    for (uint32_t f0 = 0; f0 < d.nf; f0 += NF_FG) {
+        float aE[NF_FG][6], aH[NF_FG][6];
+#pragma unroll
+        for (int g = 0; g < NF_FG; ++g) {
+            if (f0 + g >= d.nf) break;
+            const float* pE = d.accE + ((size_t)(f0 + g) * d.np + pid) * 6;
+            const float* pH = d.accH + ((size_t)(f0 + g) * d.np + pid) * 6;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { aE[g][q] = pE[q]; aH[g][q] = pH[q]; }
+        }
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const float* s = d.samp + (size_t)j * 6 * d.np + pid;
+            float E[3], Hh[3];
+#pragma unroll
+            for (int n = 0; n < 3; ++n) { E[n] = s[(size_t)n * d.np]; Hh[n] = s[(size_t)(3 + n) * d.np]; }
+            const float w = sw[j];
+#pragma unroll
+            for (int g = 0; g < NF_FG; ++g) {
+                if (f0 + g >= d.nf) break;
+                const float ce = tw[j][f0 + g][0], se = -tw[j][f0 + g][1], ch = tw[j][f0 + g][2], sh = -tw[j][f0 + g][3];
+#pragma unroll
+                for (int n = 0; n < 3; ++n) {
+                    aE[g][2 * n] = __fadd_rn(aE[g][2 * n], __fmul_rn(__fmul_rn(E[n], ce), w));
+                    aE[g][2 * n + 1] = __fadd_rn(aE[g][2 * n + 1], __fmul_rn(__fmul_rn(E[n], se), w));
+                    aH[g][2 * n] = __fadd_rn(aH[g][2 * n], __fmul_rn(__fmul_rn(Hh[n], ch), w));
+                    aH[g][2 * n + 1] = __fadd_rn(aH[g][2 * n + 1], __fmul_rn(__fmul_rn(Hh[n], sh), w));
+                }
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < NF_FG; ++g) {
+            if (f0 + g >= d.nf) break;
+            float* pE = d.accE + ((size_t)(f0 + g) * d.np + pid) * 6;
+            float* pH = d.accH + ((size_t)(f0 + g) * d.np + pid) * 6;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { pE[q] = aE[g][q]; pH[q] = aH[g][q]; }
         }
     }
 }

@@ -329,85 +329,196 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
 // UPML cells of the TMA path, outside the streaming kernel.  Their update
 // reads per-cell region coefficients and fluxes with dependent loads; run
 // inside the plane pipeline those loads stalled every CTA whose tile touches a
-// region.  k_pml_e runs before k_fused_tma and k_pml_h after it, one thread
-// per UPML cell (z fastest within a region, so accesses coalesce).  A cell
-// that several regions contain is handled once, by the first of them, with
-// the chain over all of them in region order.
+// region.  k_pml_e runs before k_fused_tma and k_pml_h after it.  A cell that
+// several regions contain is handled once, by the first of them, with the
+// chain over all of them in region order.
+//
+// Both passes are latency-bound (a z-slab region row is 8 cells, 32 bytes,
+// long), so a thread takes PML_ZC consecutive z cells of one region row and
+// issues every load of them (fields, material index and, for the usual
+// single-region cell, the region's coefficients and flux) before any
+// arithmetic.
 // ---------------------------------------------------------------------------
+constexpr uint32_t PML_ZC = 2;
 
-// Cell of flat index i over the regions' boxes; false when a lower-numbered
-// region also contains it.  `mask`: every region containing the cell.
-__device__ __forceinline__ bool pml_locate(const PmlSet& ps, uint32_t i, uint32_t& x, uint32_t& y, uint32_t& z,
-                                           uint32_t& mask) {
-    int r = 0;
-    for (; r < ps.count; ++r) {
-        const uint32_t c = ps.r[r].n[0] * ps.r[r].n[1] * ps.r[r].n[2];
-        if (i < c) break;
-        i -= c;
+// Work item i -> region r, row (x, y), first z and cell count (PML_ZC cells
+// per item along z, items in region order).
+__device__ __forceinline__ bool pml_item(const PmlSet& ps, uint32_t i, int& r, uint32_t& x, uint32_t& y, uint32_t& z,
+                                         uint32_t& cnt) {
+    for (r = 0; r < ps.count; ++r) {
+        const PmlRegion& R = ps.r[r];
+        const uint32_t zc = (R.n[2] + PML_ZC - 1) / PML_ZC;
+        const uint32_t items = R.n[0] * R.n[1] * zc;
+        if (i < items) {
+            const uint32_t row = i / zc, zi = i - row * zc;
+            x = R.s[0] + row / R.n[1];
+            y = R.s[1] + row % R.n[1];
+            z = R.s[2] + zi * PML_ZC;
+            cnt = min(PML_ZC, R.n[2] - zi * PML_ZC);
+            return true;
+        }
+        i -= items;
     }
-    if (r == ps.count) return false;
-    const PmlRegion& R = ps.r[r];
-    const uint32_t nyz = R.n[1] * R.n[2];
-    x = R.s[0] + i / nyz;
-    y = R.s[1] + (i % nyz) / R.n[2];
-    z = R.s[2] + i % R.n[2];
+    return false;
+}
+
+// Every region containing (x, y, z) when region r is the first that does, else 0.
+__device__ __forceinline__ uint32_t pml_owner_mask(const PmlSet& ps, int r, uint32_t x, uint32_t y, uint32_t z) {
     for (int q = 0; q < r; ++q)
-        if (in_region(ps.r[q], x, y, z)) return false;
-    mask = 0;
-    for (int q = r; q < ps.count; ++q)
-        if (in_region(ps.r[q], x, y, z)) mask |= 1u << q;
-    return true;
+        if (in_region(ps.r[q], x, y, z)) return 0u;
+    uint32_t m = 1u << r;
+    for (int q = r + 1; q < ps.count; ++q)
+        if (in_region(ps.r[q], x, y, z)) m |= 1u << q;
+    return m;
+}
+
+// Region coefficients and old flux of one single-region cell (3 components).
+template <bool VOLT>
+__device__ __forceinline__ void pml_fetch(const PmlRegion& R, uint32_t x, uint32_t y, uint32_t z, float a[3], float b[3],
+                                          float fn[3], float fo[3]) {
+    const size_t p0 = region_p(R, 0, x, y, z), nreg = (size_t)R.n[0] * R.n[1] * R.n[2];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+        const size_t p = p0 + n * nreg;
+        a[n] = __ldg((VOLT ? R.vv : R.ii) + p);
+        b[n] = __ldg((VOLT ? R.vvfo : R.iifo) + p);
+        fn[n] = __ldg((VOLT ? R.vvfn : R.iifn) + p);
+        fo[n] = __ldg((VOLT ? R.vflux : R.cflux) + p);
+    }
+}
+
+// The single-region chain of pml_cell on prefetched values; writes the new flux.
+template <bool VOLT>
+__device__ __forceinline__ float pml_one(const PmlRegion& Rn, size_t p, float vold, bool core, float cv, float ci, float curl,
+                                         float a, float b, float fn, float fo) {
+    const float fh = __fsub_rn(__fmul_rn(a, vold), __fmul_rn(b, fo));
+    const float v = core ? upd(fo, cv, ci, curl) : fo;
+    (VOLT ? Rn.vflux : Rn.cflux)[p] = v;
+    return __fadd_rn(fh, __fmul_rn(fn, v));
 }
 
 // E_new of the UPML cells (reads H_old and E_old, the old flux; writes the new
 // flux).  E_new is written over E_old in `V0w` (the step's old-E buffer, dead
 // after this step's core update), where k_fused_tma stages it.
 template <bool IDX>
-__global__ void k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t total) {
+__global__ void __launch_bounds__(256) k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t items) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
-    uint32_t x, y, z, mask;
-    if (!pml_locate(ps, i, x, y, z, mask)) return;
+    if (i >= items) return;
+    int r;
+    uint32_t x, y, z0, cnt;
+    if (!pml_item(ps, i, r, x, y, z0, cnt)) return;
     const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;
-    const uint32_t c = x * NyNz + y * Nz + z;
-    const uint32_t xm = x > 0 ? c - NyNz : c, ym = y > 0 ? c - Nz : c, zm = z > 0 ? c - 1 : c;   // self at index 0
+    const uint32_t c0 = x * NyNz + y * Nz + z0;
+    const uint32_t dx = x > 0 ? NyNz : 0u, dy = y > 0 ? Nz : 0u;      // x-1 / y-1 neighbour (self at index 0)
     const float* H = g.H0;
-    const float cx = curl4(H[2 * N + c], H[2 * N + ym], H[N + c], H[N + zm]);
-    const float cy = curl4(H[c], H[zm], H[2 * N + c], H[2 * N + xm]);
-    const float cz = curl4(H[N + c], H[N + xm], H[c], H[ym]);
-    float kk[6];
-    coeffs_f<IDX>(g, c, IDX ? __ldg(g.mat + c) : 0u, 0, kk);
-    const float e0 = V0w[c], e1 = V0w[N + c], e2 = V0w[2 * N + c];
-    const float n0 = pml_chain_pp<true>(ps, pn, mask, x, y, z, 0, e0, true, kk[0], kk[3], cx, true);
-    const float n1 = pml_chain_pp<true>(ps, pn, mask, x, y, z, 1, e1, true, kk[1], kk[4], cy, true);
-    const float n2 = pml_chain_pp<true>(ps, pn, mask, x, y, z, 2, e2, true, kk[2], kk[5], cz, true);
-    V0w[c] = n0; V0w[N + c] = n1; V0w[2 * N + c] = n2;
+    const PmlRegion& R = ps.r[r];
+    uint32_t mask[PML_ZC], m[PML_ZC];
+    float hv[PML_ZC][9], eo[PML_ZC][3], a[PML_ZC][3], b[PML_ZC][3], fn[PML_ZC][3], fo[PML_ZC][3];
+    // ---- every load of the item's cells
+#pragma unroll
+    for (uint32_t j = 0; j < PML_ZC; ++j) {
+        mask[j] = j < cnt ? pml_owner_mask(ps, r, x, y, z0 + j) : 0u;
+        if (!mask[j]) continue;
+        const uint32_t c = c0 + j, dz = (z0 + j) > 0 ? 1u : 0u;
+        hv[j][0] = H[c]; hv[j][1] = H[N + c]; hv[j][2] = H[2 * N + c];
+        hv[j][3] = H[2 * N + c - dy];      // hz(y-1)
+        hv[j][4] = H[N + c - dz];          // hy(z-1)
+        hv[j][5] = H[c - dz];              // hx(z-1)
+        hv[j][6] = H[2 * N + c - dx];      // hz(x-1)
+        hv[j][7] = H[N + c - dx];          // hy(x-1)
+        hv[j][8] = H[c - dy];              // hx(y-1)
+        eo[j][0] = V0w[c]; eo[j][1] = V0w[N + c]; eo[j][2] = V0w[2 * N + c];
+        m[j] = IDX ? __ldg(g.mat + c) : 0u;
+        if (mask[j] == (1u << r)) pml_fetch<true>(R, x, y, z0 + j, a[j], b[j], fn[j], fo[j]);
+    }
+    // ---- update and store
+#pragma unroll
+    for (uint32_t j = 0; j < PML_ZC; ++j) {
+        if (!mask[j]) continue;
+        const uint32_t c = c0 + j, z = z0 + j;
+        const float cv[3] = {curl4(hv[j][2], hv[j][3], hv[j][1], hv[j][4]),     // backward curl, reference order
+                             curl4(hv[j][0], hv[j][5], hv[j][2], hv[j][6]),
+                             curl4(hv[j][1], hv[j][7], hv[j][0], hv[j][8])};
+        float kk[6];
+        coeffs_f<IDX>(g, c, m[j], 0, kk);
+        float en[3];
+        if (mask[j] == (1u << r)) {
+            const size_t p0 = region_p(R, 0, x, y, z), nreg = (size_t)R.n[0] * R.n[1] * R.n[2];
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+                en[n] = pml_one<true>(pn.r[r], p0 + n * nreg, eo[j][n], true, kk[n], kk[3 + n], cv[n], a[j][n], b[j][n],
+                                      fn[j][n], fo[j][n]);
+        } else {
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+                en[n] = pml_chain_pp<true>(ps, pn, mask[j], x, y, z, n, eo[j][n], true, kk[n], kk[3 + n], cv[n], true);
+        }
+        V0w[c] = en[0]; V0w[N + c] = en[1]; V0w[2 * N + c] = en[2];
+    }
 }
 
 // H_new of the UPML cells from the final-core E_new (cells whose curl reads E
 // rewritten by a sparse operation are redone by k_deferred_h).
 template <bool IDX>
-__global__ void k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t total) {
+__global__ void __launch_bounds__(256) k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t items) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
-    uint32_t x, y, z, mask;
-    if (!pml_locate(ps, i, x, y, z, mask)) return;
+    if (i >= items) return;
+    int r;
+    uint32_t x, y, z0, cnt;
+    if (!pml_item(ps, i, r, x, y, z0, cnt)) return;
     const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;
-    const uint32_t c = x * NyNz + y * Nz + z;
-    const bool core = (x + 1 < g.Nx) && (y + 1 < g.Ny) && (z + 1 < g.Nz);
+    const uint32_t c0 = x * NyNz + y * Nz + z0;
     const float* V = g.V1;
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (core) {
-        cx = curl4(V[2 * N + c], V[2 * N + c + Nz], V[N + c], V[N + c + 1]);
-        cy = curl4(V[c], V[c + 1], V[2 * N + c], V[2 * N + c + NyNz]);
-        cz = curl4(V[N + c], V[N + c + NyNz], V[c], V[c + Nz]);
-        coeffs_f<IDX>(g, c, IDX ? __ldg(g.mat + c) : 0u, 6, kk);
+    const PmlRegion& R = ps.r[r];
+    uint32_t mask[PML_ZC], m[PML_ZC];
+    bool core[PML_ZC];
+    float ev[PML_ZC][9], ho[PML_ZC][3], a[PML_ZC][3], b[PML_ZC][3], fn[PML_ZC][3], fo[PML_ZC][3];
+    const bool core_xy = (x + 1 < g.Nx) && (y + 1 < g.Ny);
+#pragma unroll
+    for (uint32_t j = 0; j < PML_ZC; ++j) {
+        mask[j] = j < cnt ? pml_owner_mask(ps, r, x, y, z0 + j) : 0u;
+        if (!mask[j]) continue;
+        const uint32_t c = c0 + j;
+        core[j] = core_xy && (z0 + j + 1 < g.Nz);
+        if (core[j]) {
+            ev[j][0] = V[c]; ev[j][1] = V[N + c]; ev[j][2] = V[2 * N + c];
+            ev[j][3] = V[2 * N + c + Nz];      // ez(y+1)
+            ev[j][4] = V[N + c + 1];           // ey(z+1)
+            ev[j][5] = V[c + 1];               // ex(z+1)
+            ev[j][6] = V[2 * N + c + NyNz];    // ez(x+1)
+            ev[j][7] = V[N + c + NyNz];        // ey(x+1)
+            ev[j][8] = V[c + Nz];              // ex(y+1)
+            m[j] = IDX ? __ldg(g.mat + c) : 0u;
+        }
+        ho[j][0] = g.H0[c]; ho[j][1] = g.H0[N + c]; ho[j][2] = g.H0[2 * N + c];
+        if (mask[j] == (1u << r)) pml_fetch<false>(R, x, y, z0 + j, a[j], b[j], fn[j], fo[j]);
     }
-    const float h0 = pml_chain_pp<false>(ps, pn, mask, x, y, z, 0, g.H0[c], core, kk[0], kk[3], cx, true);
-    const float h1 = pml_chain_pp<false>(ps, pn, mask, x, y, z, 1, g.H0[N + c], core, kk[1], kk[4], cy, true);
-    const float h2 = pml_chain_pp<false>(ps, pn, mask, x, y, z, 2, g.H0[2 * N + c], core, kk[2], kk[5], cz, true);
-    g.H1[c] = h0; g.H1[N + c] = h1; g.H1[2 * N + c] = h2;
+#pragma unroll
+    for (uint32_t j = 0; j < PML_ZC; ++j) {
+        if (!mask[j]) continue;
+        const uint32_t c = c0 + j, z = z0 + j;
+        float cv[3] = {0.f, 0.f, 0.f};
+        float kk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (core[j]) {                        // forward curl, reference order
+            cv[0] = curl4(ev[j][2], ev[j][3], ev[j][1], ev[j][4]);
+            cv[1] = curl4(ev[j][0], ev[j][5], ev[j][2], ev[j][6]);
+            cv[2] = curl4(ev[j][1], ev[j][7], ev[j][0], ev[j][8]);
+            coeffs_f<IDX>(g, c, m[j], 6, kk);
+        }
+        float hn[3];
+        if (mask[j] == (1u << r)) {
+            const size_t p0 = region_p(R, 0, x, y, z), nreg = (size_t)R.n[0] * R.n[1] * R.n[2];
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+                hn[n] = pml_one<false>(pn.r[r], p0 + n * nreg, ho[j][n], core[j], kk[n], kk[3 + n], cv[n], a[j][n], b[j][n],
+                                       fn[j][n], fo[j][n]);
+        } else {
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+                hn[n] = pml_chain_pp<false>(ps, pn, mask[j], x, y, z, n, ho[j][n], core[j], kk[n], kk[3 + n], cv[n], true);
+        }
+        g.H1[c] = hn[0]; g.H1[N + c] = hn[1]; g.H1[2 * N + c] = hn[2];
+    }
 }
 
 }  // namespace efs

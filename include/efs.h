@@ -274,7 +274,8 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
 efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms);
 
 /* Diagnostics: kernel launches one timestep enqueues with the current
- * configuration (a captured batch of n steps adds one counter update). */
+ * configuration (a captured batch of n steps adds one counter update and,
+ * with NF2FF configured, ceil(n/16) accumulator passes). */
 efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out);
 
 #ifdef __cplusplus

@@ -344,6 +344,26 @@ def test_nf2ff_accumulation(cuda_engine_cls, window):
         assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), k
 
 
+def test_nf2ff_buffered_batches(cuda_engine_cls):
+    """Surface samples are buffered and folded into the accumulators every 16th
+    step and at each batch's end: irregular iterate() sizes (one spans two
+    captured graphs) and 5 frequencies (two register groups) must still match
+    the oracle's per-step accumulation after every call."""
+    N = (14, 13, 15)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 41, pec_frac=0))
+    cfg = nf2ff_inputs(N, nfreq=5)
+    g.configureNF2FFAccumulation(cfg)
+    o.configureNF2FFAccumulation(cfg)
+    seed_fields(g, o, N, 42)
+    for n in (1, 17, 70, 16, 5):
+        g.iterate(n)
+        o.iterate(n)
+        ag, ao = g.readNF2FFAccumulation(True), o.readNF2FFAccumulation(True)
+        for k in ("accumE", "accumH"):
+            a, b = np.asarray(ag[k], np.float64), np.asarray(ao[k], np.float64)
+            assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), (n, k)
+
+
 def test_far_field_against_f64(cuda_engine_cls):
     N = (14, 13, 15)
     g, _ = both(cuda_engine_cls, N, rand_coeffs(N, 31, pec_frac=0))
