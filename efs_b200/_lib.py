@@ -74,6 +74,13 @@ SIGNATURES = {
     "efs_energy": (C.c_int, [vp, C.c_int, f64p]),
     "efs_flush_energy": (C.c_int, [vp, f64p]),
     "efs_energy_noalloc": (C.c_int, [vp, f64p]),
+    "efs_batch_create": (C.c_int, [C.POINTER(vp), C.POINTER(vp), C.c_uint32]),
+    "efs_batch_destroy": (C.c_int, [vp]),
+    "efs_batch_last_error": (C.c_char_p, [vp]),
+    "efs_batch_iterate": (C.c_int, [vp, C.c_uint32]),
+    "efs_batch_sync": (C.c_int, [vp]),
+    "efs_batch_set_shape": (C.c_int, [vp, C.c_uint32, C.c_uint32]),
+    "efs_batch_autotune": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "efs_get_fields": (C.c_int, [vp, f32p, f32p]),
     "efs_set_fields": (C.c_int, [vp, f32p, f32p]),
     "efs_get_state": (C.c_int, [vp, vp, szt, C.POINTER(szt)]),

@@ -462,10 +462,9 @@ struct efs_engine {
             k_nf2ff_sample<<<blocks(nf.np, T), T, 0, stream>>>(V1, C1, j, nf);
             if (j == NF_K - 1 || last) k_nf2ff_flush<<<blocks(nf.np, T), T, 0, stream>>>(st, k - j, j + 1, nf);
         }
-        if (ring_on)
-            k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V1, C1, st, k, ring_idx.as<uint32_t>(), ring_n, ring_interval,
-                                                                  ring_q0, ring_max, ring.as<float>());
+        if (ring_on) k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V1, C1, st, k, ring_dev());
     }
+    RingDev ring_dev() const { return RingDev{ring_idx.as<uint32_t>(), ring_n, ring_interval, ring_q0, ring_max, ring.as<float>()}; }
 
     template <bool IDX, bool PML, int CPT, int TY>
     void launch_fused_k(dim3 g, dim3 b, const FusedGrid& fg, const PmlSet& ps, const PmlSet& pn) {
@@ -1599,3 +1598,6 @@ efs_status efs_device_bytes(const efs_engine* e, size_t* out) {
 }
 
 }  // extern "C"
+
+// batched form: several engines advanced together (same translation unit)
+#include "efs_batch.cuh"

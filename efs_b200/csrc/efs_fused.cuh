@@ -653,9 +653,8 @@ __global__ void __launch_bounds__(128) k_fused_reg(const FusedGrid g, const PmlS
 // H update of the deferred cells, after the E-side sparse operations:
 // reads the final E_new, H_old, writes H_new (with UPML), one thread per cell.
 template <bool IDX, bool PML>
-__global__ void __launch_bounds__(256) k_deferred_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, const uint32_t* cells,
-                                                    uint32_t n) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void deferred_h_body(const FusedGrid& g, const PmlSet& ps, const PmlSet& pn, const uint32_t* cells,
+                                                uint32_t n, uint32_t i) {
     if (i >= n) return;
     const uint32_t c = cells[i];
     const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;   // 3*N < 2^32
@@ -687,6 +686,11 @@ __global__ void __launch_bounds__(256) k_deferred_h(const FusedGrid g, const Pml
         else hn = core ? upd(ho[q], kk[q], kk[3 + q], cv[q]) : ho[q];
         g.H1[q * N + c] = hn;
     }
+}
+template <bool IDX, bool PML>
+__global__ void __launch_bounds__(256) k_deferred_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, const uint32_t* cells,
+                                                    uint32_t n) {
+    deferred_h_body<IDX, PML>(g, ps, pn, cells, n, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace efs

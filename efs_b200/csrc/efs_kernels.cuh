@@ -262,9 +262,11 @@ struct PointSources {
     uint32_t len, period;
 };
 
+// Thread bodies below are shared by the single-engine kernels and the
+// segmented kernels that advance several engines at once (efs_batch.cuh).
 template <int KIND>
-__global__ void k_point_sources(float* __restrict__ F, const StepState* st, uint32_t k, const PointSources s) {
-    uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void point_sources_body(float* __restrict__ F, const StepState* st, uint32_t k, const PointSources& s,
+                                                   uint32_t gi) {
     if (gi >= s.ngroups) return;
     const int64_t ts = (int64_t)st->numTS + k;
     const uint32_t t = s.target[gi];
@@ -289,6 +291,10 @@ __global__ void k_point_sources(float* __restrict__ F, const StepState* st, uint
     }
     F[t] = v;
 }
+template <int KIND>
+__global__ void k_point_sources(float* __restrict__ F, const StepState* st, uint32_t k, const PointSources s) {
+    point_sources_body<KIND>(F, st, k, s, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // A field read that the reference makes after the UPML pre-update: for a cell
 // inside a region the value there is the region's old flux.  sel 0 = field,
@@ -311,23 +317,23 @@ struct MurDev {
     float* saved;
     const float* const* vflux;
 };
-__global__ void k_mur_pre(const float* __restrict__ V, const MurDev m) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void mur_pre_body(const float* __restrict__ V, const MurDev& m, uint32_t i) {
     if (i >= m.n) return;
     float s = read_loc(V, m.vflux, m.pre_shifted[i]);
     float nv = read_loc(V, m.vflux, m.pre_normal[i]);
     m.saved[i] = __fsub_rn(s, __fmul_rn(m.coeff[i], nv));
 }
-__global__ void k_mur_post(const float* __restrict__ V, const MurDev m) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void mur_post_body(const float* __restrict__ V, const MurDev& m, uint32_t i) {
     if (i >= m.n) return;
     m.saved[i] = __fadd_rn(m.saved[i], __fmul_rn(m.coeff[i], V[m.shifted[i]]));
 }
-__global__ void k_mur_apply(float* __restrict__ V, const MurDev m) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void mur_apply_body(float* __restrict__ V, const MurDev& m, uint32_t i) {
     if (i >= m.napply) return;
     V[m.apply_target[i]] = m.saved[m.apply_src[i]];
 }
+__global__ void k_mur_pre(const float* __restrict__ V, const MurDev m) { mur_pre_body(V, m, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_mur_post(const float* __restrict__ V, const MurDev m) { mur_post_body(V, m, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_mur_apply(float* __restrict__ V, const MurDev m) { mur_apply_body(V, m, blockIdx.x * blockDim.x + threadIdx.x); }
 
 // Lorentz/Drude ADE state update (src/webgpu-fdtd.mjs:405-454), all orders
 // and directions of one field flattened into one list.
@@ -452,20 +458,31 @@ __global__ void k_pbc(float* __restrict__ F, const PbcDev p) {
 // Probe gather (src/webgpu-engine.mjs:2593-2606 direct, :2644-2665 ring).
 // Ring row = sample index derived from numTS: rows are written at
 // (numTS+1) % interval == 0, counted from configure time.
-__global__ void k_gather_ring(const float* __restrict__ V, const float* __restrict__ C, const StepState* st, uint32_t k,
-                              const uint32_t* idx, uint32_t G, uint32_t interval, uint32_t q0, uint32_t maxS, float* ring) {
+struct RingDev {
+    const uint32_t* idx;
+    uint32_t G, interval, q0, maxS;
+    float* ring;
+};
+__device__ __forceinline__ void gather_ring_body(const float* __restrict__ V, const float* __restrict__ C, const StepState* st,
+                                                 uint32_t k, const RingDev& r, uint32_t i) {
     const uint32_t ts1 = st->numTS + k + 1;
-    if (ts1 % interval != 0) return;
-    const uint32_t q = ts1 / interval;
-    if (q <= q0) return;
-    const uint32_t s = q - 1 - q0;
-    if (s >= maxS) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= G) return;
+    if (ts1 % r.interval != 0) return;
+    const uint32_t q = ts1 / r.interval;
+    if (q <= r.q0) return;
+    const uint32_t s = q - 1 - r.q0;
+    if (s >= r.maxS) return;
+    if (i >= r.G) return;
+    const uint32_t* idx = r.idx;
+    const uint32_t G = r.G;
+    float* ring = r.ring;
     const uint32_t t = idx[i];
     float* row = ring + (size_t)s * G * 2;
     row[2 * i] = V[t];
     row[2 * i + 1] = C[t];
+}
+__global__ void k_gather_ring(const float* __restrict__ V, const float* __restrict__ C, const StepState* st, uint32_t k,
+                              const RingDev r) {
+    gather_ring_body(V, C, st, k, r, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void k_gather(const float* __restrict__ V, const float* __restrict__ C, const uint32_t* idx, uint32_t G, float* out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -532,9 +549,8 @@ __device__ __forceinline__ void nf2ff_fields(const float* __restrict__ V, const 
 
 // Every step: the interpolated surface fields of the step into sample slot
 // `slot` ([slot][6][np], E then H components).
-__global__ void __launch_bounds__(256) k_nf2ff_sample(const float* __restrict__ V, const float* __restrict__ C, uint32_t slot,
-                                                      const Nf2ffDev d) {
-    const uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void nf2ff_sample_body(const float* __restrict__ V, const float* __restrict__ C, uint32_t slot,
+                                                  const Nf2ffDev& d, uint32_t pid) {
     if (pid >= d.np) return;
     float E[3], Hh[3];
     nf2ff_fields(V, C, d, pid, E, Hh);
@@ -545,6 +561,10 @@ __global__ void __launch_bounds__(256) k_nf2ff_sample(const float* __restrict__ 
         s[(size_t)(3 + n) * d.np] = Hh[n];
     }
 }
+__global__ void __launch_bounds__(256) k_nf2ff_sample(const float* __restrict__ V, const float* __restrict__ C, uint32_t slot,
+                                                      const Nf2ffDev d) {
+    nf2ff_sample_body(V, C, slot, d, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // Running DFT of `cnt` buffered steps (timesteps numTS+k0+1 .. numTS+k0+cnt,
 // WebGPUEngine.iterate passes numTS+1, :2484): each accumulator is loaded
@@ -552,7 +572,8 @@ __global__ void __launch_bounds__(256) k_nf2ff_sample(const float* __restrict__ 
 // same order, as one accumulation per step) and is stored once.  Phase per
 // step and frequency in f64 reduced mod 2*pi, then rounded to f32.
 constexpr int NF_FG = 4;   // frequencies per register group
-__global__ void __launch_bounds__(256) k_nf2ff_flush(const StepState* st, uint32_t k0, uint32_t cnt, const Nf2ffDev d) {
+// Block body: `blk` is the block's index within this NF2FF set (all threads of a block call it).
+__device__ __forceinline__ void nf2ff_flush_block(const StepState* st, uint32_t k0, uint32_t cnt, const Nf2ffDev& d, uint32_t blk) {
     __shared__ float tw[NF_K][NF_MAX_FREQ][4];
     __shared__ float sw[NF_K];
     const uint32_t ts0 = st->numTS + k0 + 1;
@@ -574,7 +595,7 @@ __global__ void __launch_bounds__(256) k_nf2ff_flush(const StepState* st, uint32
         sw[j] = __fmul_rn(__fmul_rn(ww, d.wnorm), d.dT32);
     }
     __syncthreads();
-    const uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t pid = blk * blockDim.x + threadIdx.x;
     if (pid >= d.np) return;
     for (uint32_t f0 = 0; f0 < d.nf; f0 += NF_FG) {
         float aE[NF_FG][6], aH[NF_FG][6];
@@ -614,6 +635,9 @@ __global__ void __launch_bounds__(256) k_nf2ff_flush(const StepState* st, uint32
             for (int q = 0; q < 6; ++q) { pE[q] = aE[g][q]; pH[q] = aH[g][q]; }
         }
     }
+}
+__global__ void __launch_bounds__(256) k_nf2ff_flush(const StepState* st, uint32_t k0, uint32_t cnt, const Nf2ffDev d) {
+    nf2ff_flush_block(st, k0, cnt, d, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -116,18 +116,33 @@ __device__ __forceinline__ void tt_issue(TmaSmem& S, int s, const CUtensorMap* t
     if (IDX) tma_load_3d(&S.st[s].M[0][0], tmM, z0, y0, x, bar);
 }
 
-template <bool IDX, bool PML>
-__global__ void __launch_bounds__(TT_THREADS, 2)
-k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmE,
-            const __grid_constant__ CUtensorMap tmM, const FusedGrid g, const PmlSet ps) {
+// The CTA's shared working area: 128-byte aligned, addressed from the shared
+// array itself so that every access compiles to a shared-space load or store.
+__device__ __forceinline__ TmaSmem& tt_smem() {
     extern __shared__ __align__(128) unsigned char tt_smem_raw[];
-    // 128-byte aligned working area, addressed from the shared array itself so that
-    // every access compiles to a shared-space load or store
-    TmaSmem& S = *reinterpret_cast<TmaSmem*>(tt_smem_raw + ((128u - (smem_u32(tt_smem_raw) & 127u)) & 127u));
+    return *reinterpret_cast<TmaSmem*>(tt_smem_raw + ((128u - (smem_u32(tt_smem_raw) & 127u)) & 127u));
+}
+
+// mbarrier set-up, once per CTA (all threads call it).
+__device__ __forceinline__ void tt_init(TmaSmem& S) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < TT_S; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.full[s])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// One tile of the streaming update: the x-chunk starting at xs of the tile at
+// (y0, z0), called by every thread of the CTA.  K counts the planes the CTA
+// consumed before this tile (it selects the stage, the mbarrier phase and the
+// E_new buffer, so one CTA can run tiles back to back); every load the tile
+// issues is consumed before it returns.  Returns false after a wait ran out.
+template <bool IDX, bool PML>
+__device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, const CUtensorMap* tmE, const CUtensorMap* tmM,
+                                         const FusedGrid& g, const PmlSet& ps, uint32_t xs, uint32_t y0, uint32_t z0,
+                                         uint32_t& K) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t z0 = blockIdx.x * TT_Z, y0 = blockIdx.y * TT_Y;
-    const uint32_t xs = blockIdx.z * g.xchunk;
-    if (xs >= g.Nx) return;                                  // uniform per CTA
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
     const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;           // last plane whose E this CTA computes
     const int nk = (int)(xl - xs) + 1;                       // planes streamed
@@ -166,17 +181,11 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
             for (int q = 0; q < 3; ++q) yzm[q] = axis_mask(ps, cand, 1, sy[q]) & axis_mask(ps, cand, 2, sz[q]);
     }
 
-    // ---- pipeline set-up
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int s = 0; s < TT_S; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.full[s])));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
+    // ---- first planes into the pipeline
     int issued = 0;                                          // planes issued (thread 0's count)
     if (threadIdx.x == 0)
         for (; issued < TT_S && issued < nk; ++issued)
-            tt_issue<IDX>(S, issued, &tmH, &tmE, &tmM, (int)(xs + issued), (int)y0, (int)z0);
+            tt_issue<IDX>(S, (int)((K + issued) % TT_S), tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);
 
     // H_old(xs-1) of the E cells (y, z components); at xs = 0 the x-1 neighbour is plane 0 itself
     float hp[3][3];
@@ -196,14 +205,14 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
     int k = 0;
 
     for (; k < nk; ++k) {
-        const uint32_t x = xs + k;
-        const int s = k % TT_S;
-        const bool ok = mbar_wait_bounded(smem_u32(&S.full[s]), (uint32_t)(k / TT_S) & 1u, WAIT_NS);
+        const uint32_t x = xs + k, kq = K + k;               // plane index within the tile / within the CTA
+        const int s = kq % TT_S;
+        const bool ok = mbar_wait_bounded(smem_u32(&S.full[s]), (kq / TT_S) & 1u, WAIT_NS);
         const uint32_t xmask = cand ? axis_mask(ps, cand, 0, x) : 0u;
         const float* Hs = &S.st[s].H[0][0][0];
         const float* Es = &S.st[s].E[0][0][0];
         const uint32_t* Ms = &S.st[s].M[0][0];
-        float* En = &S.En[k % 3][0][0][0];
+        float* En = &S.En[kq % 3][0][0][0];
         const uint32_t px = x * NyNz;
         float en[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
         float hc[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
@@ -261,12 +270,12 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
         timed_out = __syncthreads_or(!ok) != 0;
         if (timed_out) break;
         if (threadIdx.x == 0 && issued < nk) {
-            tt_issue<IDX>(S, s, &tmH, &tmE, &tmM, (int)(xs + issued), (int)y0, (int)z0);
+            tt_issue<IDX>(S, s, tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);   // stage of plane k+TT_S
             ++issued;
         }
         // ---- H_new(x-1) of the owned cells
         if (k > 0 && own) {
-            const float* Ep = &S.En[(k + 2) % 3][0][0][0];
+            const float* Ep = &S.En[(kq + 2) % 3][0][0][0];
             float nb[2][4], kh[2][6];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
@@ -309,9 +318,9 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
         if (threadIdx.x == 0) {
             atomicOr(g.status, 1u);
             for (int j = k; j < issued; ++j)                       // drain the loads still in flight
-                (void)mbar_wait_bounded(smem_u32(&S.full[j % TT_S]), (uint32_t)(j / TT_S) & 1u, WAIT_NS);
+                (void)mbar_wait_bounded(smem_u32(&S.full[(K + j) % TT_S]), ((K + j) / TT_S) & 1u, WAIT_NS);
         }
-        return;
+        return false;
     }
     // ---- H of the last plane x = Nx-1: no core update (pass-through; UPML cells: k_pml_h)
     if (xe == g.Nx && own) {
@@ -323,6 +332,20 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
             for (int n = 0; n < 3; ++n) H1[off[q] + n * N] = hp[q][n];
         }
     }
+    K += nk;
+    return true;
+}
+
+template <bool IDX, bool PML>
+__global__ void __launch_bounds__(TT_THREADS, 2)
+k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmE,
+            const __grid_constant__ CUtensorMap tmM, const FusedGrid g, const PmlSet ps) {
+    const uint32_t xs = blockIdx.z * g.xchunk;
+    if (xs >= g.Nx) return;                                  // uniform per CTA
+    TmaSmem& S = tt_smem();
+    tt_init(S);
+    uint32_t K = 0;
+    (void)tma_tile<IDX, PML>(S, &tmH, &tmE, &tmM, g, ps, xs, blockIdx.y * TT_Y, blockIdx.x * TT_Z, K);
 }
 
 // ---------------------------------------------------------------------------
@@ -401,8 +424,8 @@ __device__ __forceinline__ float pml_one(const PmlRegion& Rn, size_t p, float vo
 // flux).  E_new is written over E_old in `V0w` (the step's old-E buffer, dead
 // after this step's core update), where k_fused_tma stages it.
 template <bool IDX>
-__global__ void __launch_bounds__(256) k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t items) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pml_e_body(const FusedGrid& g, const PmlSet& ps, const PmlSet& pn, float* V0w, uint32_t items,
+                                           uint32_t i) {
     if (i >= items) return;
     int r;
     uint32_t x, y, z0, cnt;
@@ -456,12 +479,15 @@ __global__ void __launch_bounds__(256) k_pml_e(const FusedGrid g, const PmlSet p
         V0w[c] = en[0]; V0w[N + c] = en[1]; V0w[2 * N + c] = en[2];
     }
 }
+template <bool IDX>
+__global__ void __launch_bounds__(256) k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t items) {
+    pml_e_body<IDX>(g, ps, pn, V0w, items, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // H_new of the UPML cells from the final-core E_new (cells whose curl reads E
 // rewritten by a sparse operation are redone by k_deferred_h).
 template <bool IDX>
-__global__ void __launch_bounds__(256) k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t items) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pml_h_body(const FusedGrid& g, const PmlSet& ps, const PmlSet& pn, uint32_t items, uint32_t i) {
     if (i >= items) return;
     int r;
     uint32_t x, y, z0, cnt;
@@ -519,6 +545,10 @@ __global__ void __launch_bounds__(256) k_pml_h(const FusedGrid g, const PmlSet p
         }
         g.H1[c] = hn[0]; g.H1[N + c] = hn[1]; g.H1[2 * N + c] = hn[2];
     }
+}
+template <bool IDX>
+__global__ void __launch_bounds__(256) k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t items) {
+    pml_h_body<IDX>(g, ps, pn, items, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace efs

@@ -449,3 +449,45 @@ class CudaEngine:
         out = np.zeros(cnt.value, np.float32)
         self._ck(self._lib.efs_debug_read(self._h, name.encode(), int(arg), _p(out, C.c_float), out.size, C.byref(cnt)))
         return out
+
+
+class CudaBatch:
+    """Batched form (efs_batch_*): several configured CudaEngine objects of one
+    device advanced together by one persistent fused-update launch and one
+    launch per sparse phase.  Members keep their own step counters and stay
+    usable through their own methods between batch calls."""
+
+    def __init__(self, engines):
+        self._lib = _lib.load()
+        self.members = list(engines)
+        arr = (C.c_void_p * len(self.members))(*[e.handle for e in self.members])
+        h = C.c_void_p()
+        rc = self._lib.efs_batch_create(C.byref(h), arr, len(self.members))
+        if rc != 0:
+            raise EfsError(rc, self._lib.efs_batch_last_error(None).decode())
+        self._h = h
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise EfsError(rc, self._lib.efs_batch_last_error(self._h).decode())
+
+    def iterate(self, n):
+        self._ck(self._lib.efs_batch_iterate(self._h, int(n)))
+
+    def sync(self):
+        self._ck(self._lib.efs_batch_sync(self._h))
+
+    def setShape(self, xchunk, ctas_per_sm=2):
+        self._ck(self._lib.efs_batch_set_shape(self._h, int(xchunk), int(ctas_per_sm)))
+
+    def autotune(self, steps=16):
+        """Pick plane depth and CTAs per SM by timing real steps (advances the
+        members by 17*steps timesteps; results are the same under every shape)."""
+        x, c, ms = C.c_uint32(), C.c_uint32(), C.c_float()
+        self._ck(self._lib.efs_batch_autotune(self._h, int(steps), C.byref(x), C.byref(c), C.byref(ms)))
+        return {"xchunk": x.value, "ctas_per_sm": c.value, "ms_per_step": ms.value}
+
+    def destroy(self):
+        if self._h is not None:
+            self._lib.efs_batch_destroy(self._h)
+            self._h = None

@@ -278,6 +278,36 @@ efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms);
  * with NF2FF configured, ceil(n/16) accumulator passes). */
 efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out);
 
+/* --- batched form ------------------------------------------------------
+ * No counterpart in the reference (its sweeps run one solve after another).
+ * A batch advances several configured engines of one device together: one
+ * persistent fused-update launch over a work-tile list spanning every
+ * member, one launch per sparse phase for all members, up to 64 steps per
+ * captured CUDA graph.  Each member computes exactly what it computes alone
+ * and keeps its own step counter; between batch calls each member stays
+ * usable through the per-engine calls (probe reads, energy, fields).  Members
+ * need the TMA-fed fused path (Nz a multiple of 4) and may use excitation,
+ * Mur, TFSF, UPML, NF2FF and the probe ring (not steady state, ADE, RLC,
+ * PBC); members may mix material-index and dense coefficients.  Stepping
+ * or reconfiguring a member on its own between batch calls is allowed: the
+ * batch re-plans. */
+typedef struct efs_batch efs_batch;
+efs_status efs_batch_create(efs_batch** out, efs_engine* const* engines, uint32_t count);
+efs_status efs_batch_destroy(efs_batch* b);
+const char* efs_batch_last_error(const efs_batch* b);
+/* Advance every member n timesteps (ordered after and before the members'
+ * own stream work; returns without waiting). */
+efs_status efs_batch_iterate(efs_batch* b, uint32_t n);
+efs_status efs_batch_sync(efs_batch* b);
+/* Plane depth (x-planes per work tile) and resident CTAs per SM (1 or 2) of
+ * the persistent launch; results do not depend on them. */
+efs_status efs_batch_set_shape(efs_batch* b, uint32_t xchunk, uint32_t ctas_per_sm);
+/* Autotuner: times `steps` real timesteps for each candidate shape (plane
+ * depth 8/16/32/64 x 1-2 CTAs per SM), keeps the fastest and reports it.
+ * The timed steps advance the members (bit-identical under every shape):
+ * the batch moves forward by 17*steps timesteps in all. */
+efs_status efs_batch_autotune(efs_batch* b, uint32_t steps, uint32_t* xchunk, uint32_t* ctas_per_sm, float* ms_per_step);
+
 #ifdef __cplusplus
 }
 #endif
