@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--n", type=int, default=512, help="grid lines per axis")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-timesteps", type=int, default=2, help="timesteps per reference-arm step")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-sweep measurement")
+    p.add_argument("--batch-count", type=int, default=64, help="instances of the batched sweep")
     return p.parse_args()
 
 
@@ -192,6 +194,54 @@ def run_reference(args):
     }))
 
 
+def batched_sweep(args, local):
+    """Batched form on the stub-filter sweep (64 microstrip filters, uneven
+    grids): every member advanced by one persistent fused launch per timestep
+    (efs_batch_*), against the same engines stepped one after another.  Both
+    legs run the same number of timesteps per member (graphs captured in an
+    identical warm-up leg) and are timed by the wall clock around
+    device-synchronised runs."""
+    from efs_b200 import workloads
+    from efs_b200.engine import CudaBatch, CudaEngine
+    jobs = workloads.stub_filters(count=args.batch_count)
+    engines = []
+    for j in jobs:
+        e = CudaEngine(device=local)
+        e.initGPU()
+        workloads.configure(e, j)
+        engines.append(e)
+    cells = sum(j["grid"][0] * j["grid"][1] * j["grid"][2] for j in jobs)
+    b = CudaBatch(engines)
+    tuned = b.autotune(steps=8)                  # real timesteps, identical results under every shape
+    T = 192                                      # timesteps per member in each timed leg (3 graphs of 64)
+    b.iterate(T)
+    b.sync()
+    t0 = time.perf_counter()
+    b.iterate(T)
+    b.sync()
+    t_batch = time.perf_counter() - t0
+    for e in engines:                            # sequential: one engine after another, each its own graphs
+        e.iterate(T)
+    for e in engines:
+        e.sync()
+    t0 = time.perf_counter()
+    for e in engines:
+        e.iterate(T)
+        e.sync()
+    t_seq = time.perf_counter() - t0
+    b.destroy()
+    for e in engines:
+        e.destroy()
+    v_b = cells * T / t_batch / 1e6
+    v_s = cells * T / t_seq / 1e6
+    return {"workload": "stub_filters x%d: per-axis U[60,180] lines, 0.2 mm, Mur, two 50-ohm ports" % len(jobs),
+            "instances": len(jobs), "cells": cells, "timesteps_per_member": T,
+            "batched_mcells_s": round(v_b, 1), "sequential_mcells_s": round(v_s, 1), "speedup": round(v_b / v_s, 3),
+            "batched_solves_per_s_15000_steps": round(v_b * 1e6 / (cells / len(jobs)) / 15000, 3),
+            "sequential_solves_per_s_15000_steps": round(v_s * 1e6 / (cells / len(jobs)) / 15000, 3),
+            "autotuned": tuned, "timing": "wall clock around device-synchronised runs of %d timesteps" % T}
+
+
 def run_b200(args):
     import torch
     rank, local, world = dist_env()
@@ -301,6 +351,9 @@ def run_b200(args):
         v, threads, dt = cpu_sample(job, "js", 2)
         cpu = {"value": round(v, 3), "unit": "MCells/s", "cores": threads, "kind": "port",
                "sample": "2 timesteps of the same %d^3 job on the CPU oracle (CPUFDTDEngine arithmetic), %.1f s" % (args.n, dt)}
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_sweep(args, local)
     if rank == 0:
         print(json.dumps({
             "metric": "MCells/s", "value": round(value, 3), "unit": "MCells/s", "n_gpus": world,
@@ -317,6 +370,7 @@ def run_b200(args):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk.summary(),
+            "batched": batched,
         }))
     if world > 1:
         import torch.distributed as dist

@@ -159,6 +159,76 @@ def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_ins
     return job
 
 
+def _stub_filter_one(args):
+    """Coefficients of one microstrip stub filter (runs in a worker)."""
+    grid, delta, dT, sub, w, stub, xa, xb, yc = args
+    Nx, Ny, Nz = grid
+    lines = [opgen.uniform_lines(N, delta) for N in grid]
+    mesh = opgen.Mesh(*lines)
+    eps = np.ones((Nx - 1, Ny - 1, Nz - 1))
+    eps[:, :, :sub] = 3.66                        # substrate on the ground plane
+    X, Y, Z = lines
+    y0t = yc - w // 2
+    xs = Nx // 2 - w // 2
+    zt = Z[sub]
+    pec = []
+    for n in range(3):
+        m = np.zeros(grid, bool)
+        if n < 2:                                 # trace and stub: sheets in the plane z = sub
+            m |= opgen.edge_mask_in_box(mesh, n, (X[xa], Y[y0t], zt), (X[xb], Y[y0t + w], zt))
+            m |= opgen.edge_mask_in_box(mesh, n, (X[xs], Y[y0t + w], zt), (X[xs + w], Y[y0t + w + stub], zt))
+        pec.append(m)
+    lumped = [np.zeros(grid) for _ in range(3)]
+    for xp in (xa, xb):                           # 50 ohm ports: `sub` series z edges between ground and trace
+        lumped[2][xp, yc, :sub] = sub / 50.0
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, eps_r=eps, pec_edges=pec, lumped_g=lumped, bc=(0, 0, 0, 0, 0, 0))
+    mat, mt = opgen.to_indexed(vv, vi, ii, iv)
+    return mat, mt.table()
+
+
+def stub_filters(count=64, seed=3, delta=0.2e-3, steps=15000, workers=None):
+    """Batched sweep: `count` microstrip stub filters with
+    per-axis line counts ~ U[60, 180] (numpy default_rng(seed); Nz rounded up
+    to a multiple of 4, which the TMA-fed kernel needs), uniform `delta` mesh
+    (so every instance shares dT and the excitation signal).  PEC ground on
+    the z = 0 face, a 0.8 mm substrate eps_r = 3.66, a 1.8 mm PEC trace along
+    x with a stub along +y of seeded length U[8, 20] mm (cut to the room the
+    grid leaves), two single-column 50 ohm lumped ports at the trace ends, a
+    Gaussian pulse f0 = fc = 3.5 GHz (0-7 GHz) driving port 1, voltage and
+    current probes at both ports, Mur ABC on the other five faces."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(60, 181, (count, 3))
+    sizes[:, 2] = (sizes[:, 2] + 3) // 4 * 4
+    stub_mm = rng.uniform(8e-3, 20e-3, count)
+    sub = int(round(0.8e-3 / delta))
+    w = int(round(1.8e-3 / delta))
+    dT = opgen.cfl_dt(opgen.Mesh(*[opgen.uniform_lines(4, delta)] * 3))
+    sig = opgen.gauss_signal(3.5e9, 3.5e9, dT, steps).astype(np.float32)
+    interval = opgen.nyquist_interval(7e9, dT)
+    items, jobs = [], []
+    for i in range(count):
+        Nx, Ny, Nz = (int(v) for v in sizes[i])
+        xa, xb, yc = 6, Nx - 7, Ny // 2
+        stub = max(1, min(int(round(stub_mm[i] / delta)), Ny - (yc - w // 2 + w) - 4))
+        items.append(((Nx, Ny, Nz), delta, dT, sub, w, stub, xa, xb, yc))
+        mesh = opgen.Mesh(*[opgen.uniform_lines(N, delta) for N in (Nx, Ny, Nz)])
+        pos = [xa * Ny * Nz + yc * Nz + z for z in range(sub)]
+        probes = []
+        for xp in (xa, xb):
+            probes.append(opgen.voltage_probe(mesh, (xp, yc, 0), (xp, yc, sub), interval=interval))
+            probes.append(opgen.current_probe(mesh, (xp - 1, yc - 1, sub // 2), (xp, yc, sub // 2), 2, interval=interval))
+        jobs.append(dict(name="stub_filter_%d" % i, grid=[Nx, Ny, Nz], dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+                         excitation=dict(signal=sig, delay=[0] * sub, amp=[1.0 / sub] * sub, dir=[2] * sub, pos=pos,
+                                         period=0),
+                         mur=opgen.mur_dual(mesh, dT, [(0, "lo"), (0, "hi"), (1, "lo"), (1, "hi"), (2, "hi")]),
+                         probes=probes, stub_cells=stub))
+    if workers is None:
+        workers = min(count, max(1, os.cpu_count() or 1), 32)
+    for job, (mat, table) in zip(jobs, _parallel_map(_stub_filter_one, items, workers)):
+        job["coefficients"] = dict(mat=mat, table=table)
+    return jobs
+
+
 def job_bytes_per_step(job):
     """Algorithmic HBM bytes of one timestep of `job` (fields read+written once,
     one u32 material index per cell, UPML/Mur/TFSF/NF2FF/probe traffic):
