@@ -1,10 +1,13 @@
-"""Small, self-terminating run of the headline workload for profilers.
+"""Small, self-terminating runs of the benchmark workloads for profilers.
 
     python -m efs_b200.profile_case --n 256 --steps 4
+    python -m efs_b200.profile_case --batch 64 --steps 4
 
-builds workloads.large_plain(n) (n^3 lines: same features as the benchmark),
-configures the CUDA engine and runs `steps` timesteps, printing the mean
-device time per timestep.  Sized by --n so a profiler capture stays small.
+The first builds workloads.large_plain(n) (n^3 lines: same features as the
+headline benchmark), configures the CUDA engine and runs `steps` timesteps,
+printing the mean device time per timestep.  --batch N instead builds the
+first N stub filters of the batched sweep (workloads.stub_filters) and runs
+them as one batch.  Sized by --n / --batch so a profiler capture stays small.
 """
 import argparse
 import time
@@ -13,6 +16,7 @@ import time
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=0, help="run N stub filters as one batch instead")
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--time-core", type=int, default=0, help="also time N launches of the core kernel(s) alone")
@@ -20,7 +24,29 @@ def main():
     from efs_b200.build import build
     build()
     from efs_b200 import workloads
-    from efs_b200.engine import CudaEngine
+    from efs_b200.engine import CudaBatch, CudaEngine
+    if args.batch:
+        jobs = workloads.stub_filters(count=args.batch)
+        engines = []
+        for j in jobs:
+            e = CudaEngine()
+            e.initGPU()
+            workloads.configure(e, j)
+            engines.append(e)
+        b = CudaBatch(engines)
+        b.iterate(args.warmup)
+        b.sync()
+        t = time.perf_counter()
+        b.iterate(args.steps)
+        b.sync()
+        dt = (time.perf_counter() - t) / max(1, args.steps)
+        N = sum(j["grid"][0] * j["grid"][1] * j["grid"][2] for j in jobs)
+        print("batch=%d cells=%d steps=%d  %.3f ms/timestep  %.1f MCells/s" % (args.batch, N, args.steps, dt * 1e3,
+                                                                             N / dt / 1e6))
+        b.destroy()
+        for e in engines:
+            e.destroy()
+        return
     job = workloads.large_plain(args.n)
     eng = CudaEngine()
     if not eng.initGPU():

@@ -187,7 +187,7 @@ def _stub_filter_one(args):
 
 
 def stub_filters(count=64, seed=3, delta=0.2e-3, steps=15000, workers=None):
-    """Batched sweep: `count` microstrip stub filters with
+    """The batched sweep workload: `count` microstrip stub filters with
     per-axis line counts ~ U[60, 180] (numpy default_rng(seed); Nz rounded up
     to a multiple of 4, which the TMA-fed kernel needs), uniform `delta` mesh
     (so every instance shares dT and the excitation signal).  PEC ground on
@@ -227,6 +227,73 @@ def stub_filters(count=64, seed=3, delta=0.2e-3, steps=15000, workers=None):
     for job, (mat, table) in zip(jobs, _parallel_map(_stub_filter_one, items, workers)):
         job["coefficients"] = dict(mat=mat, table=table)
     return jobs
+
+
+def _served_tfsf_one(args):
+    """Coefficients of one served TFSF job: vacuum cube with a dielectric box (runs in a worker)."""
+    side, nz, delta, dT = args
+    grid = (side, side, nz)
+    mesh = opgen.Mesh(*[opgen.uniform_lines(N, delta) for N in grid])
+    eps = np.ones((side - 1, side - 1, nz - 1))
+    a, b = side // 2 - side // 8, side // 2 + side // 8
+    c, d = nz // 2 - nz // 8, nz // 2 + nz // 8
+    eps[a:b, a:b, c:d] = 4.0
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, eps_r=eps, bc=(0, 0, 0, 0, 0, 0))
+    mat, mt = opgen.to_indexed(vv, vi, ii, iv)
+    return mat, mt.table()
+
+
+def served_template(kind, side, delta=0.5e-3, steps=25000):
+    """Inputs of one request of the served stream, for a cubic grid of
+    `side` lines (Nz rounded up to a multiple of 4): kind "port" is a stub
+    filter (two 50 ohm lumped ports, Mur on five faces, Gaussian 0-7 GHz at
+    port 1, probes at both ports); kind "tfsf" is a vacuum cube holding a
+    dielectric box (eps_r = 4), a TFSF Gaussian plane wave (normal incidence,
+    10 GHz +- 5 GHz) on the box 6 cells in, NF2FF on the box 3 cells in at 2
+    frequencies, Mur on all six faces.  The signal covers `steps` timesteps;
+    a request runs its own step count on these inputs."""
+    nz = (side + 3) // 4 * 4
+    if kind == "port":
+        sub, w = 4, 9
+        d = 0.2e-3                                   # port jobs keep the stub filters' 0.2 mm cells
+        dT = opgen.cfl_dt(opgen.Mesh(*[opgen.uniform_lines(4, d)] * 3))
+        xa, xb, yc = 6, side - 7, side // 2
+        stub = max(1, min(side // 3, side - (yc - w // 2 + w) - 4))
+        grid = (side, side, nz)
+        mat, table = _stub_filter_one((grid, d, dT, sub, w, stub, xa, xb, yc))
+        mesh = opgen.Mesh(*[opgen.uniform_lines(N, d) for N in grid])
+        sig = opgen.gauss_signal(3.5e9, 3.5e9, dT, steps).astype(np.float32)
+        interval = opgen.nyquist_interval(7e9, dT)
+        probes = []
+        for xp in (xa, xb):
+            probes.append(opgen.voltage_probe(mesh, (xp, yc, 0), (xp, yc, sub), interval=interval))
+            probes.append(opgen.current_probe(mesh, (xp - 1, yc - 1, sub // 2), (xp, yc, sub // 2), 2, interval=interval))
+        pos = [xa * side * nz + yc * nz + z for z in range(sub)]
+        return dict(name="served_port_%d" % side, grid=list(grid), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+                    coefficients=dict(mat=mat, table=table), probes=probes,
+                    excitation=dict(signal=sig, delay=[0] * sub, amp=[1.0 / sub] * sub, dir=[2] * sub, pos=pos, period=0),
+                    mur=opgen.mur_dual(mesh, dT, [(0, "lo"), (0, "hi"), (1, "lo"), (1, "hi"), (2, "hi")]))
+    grid = (side, side, nz)
+    mesh = opgen.Mesh(*[opgen.uniform_lines(N, delta) for N in grid])
+    dT = opgen.cfl_dt(mesh)
+    mat, table = _served_tfsf_one((side, nz, delta, dT))
+    f0, fc = 10e9, 5e9
+    sig = opgen.gauss_signal(f0, fc, dT, steps).astype(np.float32)
+
+    def coef_at(kind_, comp, flat):
+        return table[mat[flat], (3 if kind_ == "E" else 9) + comp].astype(np.float64)
+    lo, hi = [6] * 3, [side - 7, side - 7, nz - 7]
+    vp, cp = opgen.tfsf_plane_wave(mesh, dT, lo, hi, (0, 0, 1), (1, 0, 0), coef_at, len(sig))
+    pts, meta, primal, dual = opgen.nf2ff_box(mesh, [3] * 3, [side - 4, side - 4, nz - 4])
+    freqs = [f0 - fc / 2, f0 + fc / 2]
+    faces = [(a, s_) for a in range(3) for s_ in ("lo", "hi")]
+    return dict(name="served_tfsf_%d" % side, grid=list(grid), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+                coefficients=dict(mat=mat, table=table), probes=[],
+                mur=opgen.mur_dual(mesh, dT, faces),
+                tfsf=dict(signal=sig, period=0, voltagePoints=vp, currentPoints=cp),
+                nf2ff=dict(surfaceIndices=pts.ravel(), numPoints=len(pts), omegas=[2 * math.pi * f for f in freqs], dT=dT,
+                           gridSize=list(grid), primalEdgeLens=primal, dualEdgeLens=dual, maxTS=steps, windowType=0),
+                nf2ff_meta=meta, nf2ff_freqs=freqs)
 
 
 def job_bytes_per_step(job):
