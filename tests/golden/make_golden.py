@@ -7,6 +7,9 @@ the outputs are committed so the tests never read the reference tree.
                           probe voltage vp, 251 samples every 2 steps from t=0
   openems_cavity_t.npy    the matching sample times (s)
   constants.json          physical constants of the fixtures
+  coax_ports.npz          coax/reference.json: port voltage and current series
+                          (time_s, values), the analytic Z0 and the tolerance band
+                          the reference's port test applies (tests/test_api.mjs:585-620)
 """
 import json
 import os
@@ -27,4 +30,10 @@ np.save(os.path.join(OUT, "openems_cavity_vp.npy"), np.asarray(basic["voltage"],
 np.save(os.path.join(OUT, "openems_cavity_t.npy"), np.asarray(basic["time_s"], np.float64))
 with open(os.path.join(fx, "constants.json")) as f, open(os.path.join(OUT, "constants.json"), "w") as g:
     g.write(f.read())
+coax = json.load(open(os.path.join(fx, "coax", "reference.json")))
+np.savez(os.path.join(OUT, "coax_ports.npz"),
+         ut_time=np.asarray(coax["probe_ut1"]["time_s"], np.float64), ut=np.asarray(coax["probe_ut1"]["voltage"], np.float64),
+         it_time=np.asarray(coax["probe_it1"]["time_s"], np.float64), it=np.asarray(coax["probe_it1"]["voltage"], np.float64),
+         z0=np.float64(coax["Z0_analytical_ohm"]), tol_upper=np.float64(coax["tolerances"]["upper_error"]),
+         tol_lower=np.float64(coax["tolerances"]["lower_error"]))
 print("wrote", OUT)
