@@ -159,6 +159,88 @@ def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_ins
     return job
 
 
+def _graded_axis(core, count, dmax=2e-3, ratio=1.4, below=None):
+    """`core` lines (sorted, metres) extended at both ends by cells growing by
+    `ratio` up to dmax until the axis holds exactly `count` lines; `below`
+    fixes how many of the added lines go before the core (default: half)."""
+    core = list(core)
+    add = count - len(core)
+    lo_n = add // 2 if below is None else below
+    hi_n = add - lo_n
+    lo, hi = [], []
+    d = core[1] - core[0]
+    x = core[0]
+    for _ in range(lo_n):
+        d = min(d * ratio, dmax)
+        x -= d
+        lo.append(x)
+    d = core[-1] - core[-2]
+    x = core[-1]
+    for _ in range(hi_n):
+        d = min(d * ratio, dmax)
+        x += d
+        hi.append(x)
+    return np.asarray(lo[::-1] + core + hi)
+
+
+def patch_antenna(steps=30000, end_db=-50.0, pml=8):
+    """Plain single solve on a graded mesh: a patch antenna, 86 x 87 x 71 lines.
+    Cells 0.508-2 mm, graded by at most 1.4: uniform 1 mm lines over the
+    60 x 60 mm substrate footprint (patch edges, feed and centre on lines),
+    three 0.508 mm cells through the 1.524 mm substrate (eps_r 3.38,
+    0.0015 S/m), growing to 2 mm outside.  PEC ground sheet at z = 0 under the
+    substrate, 32 x 40 mm PEC patch sheet on top, a 50 ohm lumped port from
+    ground to patch at (-6, 0) mm driven by a Gaussian f0 = 2 GHz, fc = 1 GHz,
+    `pml`-cell UPML on all faces, voltage and current probes at the port every
+    step, `steps` timesteps or the energy end criterion `end_db`."""
+    mm = 1e-3
+    fine = [i * mm for i in range(-30, 31)]                 # 61 lines, 1 mm
+    X = _graded_axis(fine, 86)
+    Y = _graded_axis(fine, 87)
+    zsub = [0.0, 0.508 * mm, 1.016 * mm, 1.524 * mm]
+    Z = _graded_axis(zsub, 71, below=16)
+    mesh = opgen.Mesh(X, Y, Z)
+    Nx, Ny, Nz = mesh.shape
+    dT = opgen.cfl_dt(mesh)
+    # substrate cells
+    ix0, ix1 = mesh.snap(0, -30 * mm), mesh.snap(0, 30 * mm)
+    iy0, iy1 = mesh.snap(1, -30 * mm), mesh.snap(1, 30 * mm)
+    iz0, iz1 = mesh.snap(2, 0.0), mesh.snap(2, 1.524 * mm)
+    eps = np.ones((Nx - 1, Ny - 1, Nz - 1))
+    kap = np.zeros((Nx - 1, Ny - 1, Nz - 1))
+    eps[ix0:ix1, iy0:iy1, iz0:iz1] = 3.38
+    kap[ix0:ix1, iy0:iy1, iz0:iz1] = 0.0015
+    pec = []
+    for n in range(3):
+        m = np.zeros(mesh.shape, bool)
+        if n < 2:
+            m |= opgen.edge_mask_in_box(mesh, n, (-30 * mm, -30 * mm, 0.0), (30 * mm, 30 * mm, 0.0))            # ground
+            m |= opgen.edge_mask_in_box(mesh, n, (-16 * mm, -20 * mm, 1.524 * mm), (16 * mm, 20 * mm, 1.524 * mm))  # patch
+        pec.append(m)
+    fx, fy = mesh.snap(0, -6 * mm), mesh.snap(1, 0.0)
+    nport = iz1 - iz0
+    lumped = [np.zeros(mesh.shape) for _ in range(3)]
+    lumped[2][fx, fy, iz0:iz1] = nport / 50.0
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, eps_r=eps, kappa=kap, pec_edges=pec, lumped_g=lumped,
+                                          bc=(0, 0, 0, 0, 0, 0))
+    W = pml
+    boxes = [((0, 0, 0), (W, Ny, Nz)), ((Nx - W, 0, 0), (W, Ny, Nz)),
+             ((W, 0, 0), (Nx - 2 * W, W, Nz)), ((W, Ny - W, 0), (Nx - 2 * W, W, Nz)),
+             ((W, W, 0), (Nx - 2 * W, Ny - 2 * W, W)), ((W, W, Nz - W), (Nx - 2 * W, Ny - 2 * W, W))]
+    sig_fns = [opgen.pml_sigma(mesh, a, W, W) for a in range(3)]
+    regions = opgen.upml_apply(mesh, dT, boxes, sig_fns, vv, vi, ii, iv, build=True)
+    mat, mt = opgen.to_indexed(vv, vi, ii, iv)
+    sig = opgen.gauss_signal(2e9, 1e9, dT, steps).astype(np.float32)
+    pos = [fx * Ny * Nz + fy * Nz + z for z in range(iz0, iz1)]
+    zm = (iz0 + iz1) // 2
+    probes = [opgen.voltage_probe(mesh, (fx, fy, iz0), (fx, fy, iz1), interval=1),
+              opgen.current_probe(mesh, (fx - 1, fy - 1, zm), (fx, fy, zm), 2, interval=1)]
+    return dict(name="patch_antenna", grid=[Nx, Ny, Nz], dT=dT, maxTS=steps, endCrit=10.0 ** (end_db / 10.0),
+                mesh=mesh, coefficients=dict(mat=mat, table=mt.table()), pml=regions, probes=probes,
+                excitation=dict(signal=sig, delay=[0] * nport, amp=[1.0 / nport] * nport, dir=[2] * nport, pos=pos,
+                                period=0))
+
+
 def _stub_filter_one(args):
     """Coefficients of one microstrip stub filter (runs in a worker)."""
     grid, delta, dT, sub, w, stub, xa, xb, yc = args
