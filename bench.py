@@ -24,7 +24,6 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
 import threading
 import time
 
@@ -50,27 +49,13 @@ def parse():
     return p.parse_args()
 
 
-def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+from efs_b200.replicas import barrier_fn, dist_env, init_group, max_over_ranks, share, whole_job_rate
 
 
 def build_job(n, rank, world, barrier):
     """Rank 0 builds the seeded job; other ranks load rank 0's copy."""
     from efs_b200 import workloads
-    if world == 1:
-        return workloads.large_plain(n)
-    path = os.path.join(tempfile.gettempdir(), "efs_bench_job_%d.pkl" % n)
-    import pickle
-    if rank == 0:
-        job = workloads.large_plain(n)
-        with open(path + ".tmp", "wb") as f:
-            pickle.dump(job, f, protocol=4)
-        os.replace(path + ".tmp", path)
-    barrier()
-    if rank != 0:
-        with open(path, "rb") as f:
-            job = pickle.load(f)
-    return job
+    return share(lambda: workloads.large_plain(n), "bench_job_%d" % n, rank, world, barrier)
 
 
 class Clocks:
@@ -247,12 +232,8 @@ def run_b200(args):
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        barrier = lambda: dist.barrier()
-    else:
-        barrier = lambda: None
+        init_group("nccl", timeout_s=600)
+    barrier = barrier_fn(world)
     from efs_b200.build import build
     if rank == 0:
         build()
@@ -288,13 +269,9 @@ def run_b200(args):
     eng.sync()
     barrier()
     torch.cuda.synchronize()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, device="cuda")
     steps_total = args.steps * BATCH
-    value = world * N * steps_total / (ms_max / 1e3) / 1e6
+    value = whole_job_rate(N, steps_total, ms_max, world)
 
     # dominant kernel (the fused E+H update) timed alone with CUDA events on the engine stream
     core_ms = eng.timeCore(20)               # [fused kernel, UPML-cell passes around it]
