@@ -91,7 +91,7 @@ struct efs_engine {
     DevBuf volt_b, curr_b;      // second buffers of the fused path (parity 1)
     bool fused = true;          // single-pass E+H kernel (else separate E and H sweeps)
     int cur = 0;                // parity holding the current fields
-    uint32_t xchunk = 64;       // x-planes per block of the fused kernel
+    uint32_t xchunk = 32;       // x-planes per block of the fused kernel (EFS_XCHUNK)
     int cpt = 1;                // z cells per thread of the fused kernel (1 or 2)
     int ty_rows = 8;            // y rows per tile of the shared-memory fused kernel (8 or 16)
     int fused_kind = 2;         // 2: TMA-fed fused kernel (needs Nz % 4 == 0, else 0), 0: register-blocked, 1: shared-memory tiled
@@ -155,6 +155,7 @@ struct efs_engine {
     DevBuf rlc_gtarget, rlc_goff, rlc_type, rlc_p, rlc_vdn, rlc_jn, rlc_vil;
     uint32_t rlc_n = 0, rlc_groups = 0;
     std::vector<uint32_t> rlc_perm;   // device element order -> caller's element order
+    std::vector<uint32_t> mur_perm;   // device Mur entry order -> caller's entry order
 
     // steady state
     bool ss_on = false, ss_recording = false;
@@ -917,9 +918,22 @@ efs_status efs_configure_mur(efs_engine* e, const float* coeff, const uint32_t* 
         if (n && (!coeff || !normal || !shifted)) fail(EFS_ERR_INVALID, "Mur arrays must be non-null");
         e->check_idx3(normal, n, "Mur normal_idx");
         e->check_idx3(shifted, n, "Mur shifted_idx");
-        e->h_mur_normal.assign(normal, normal + n);
-        e->h_mur_shifted.assign(shifted, shifted + n);
-        // apply: last writer per target wins (sequential loop :1016-1023)
+        // Entries are kept in field-index order on the device, so neighbouring
+        // threads touch neighbouring cells (the caller's face order walks a
+        // face across rows).  The pre and post updates are per entry; apply
+        // resolves each target to its last writer in the caller's order
+        // (sequential loop :1016-1023), which the permutation leaves intact.
+        std::vector<uint32_t> perm(n);
+        for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+        std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) { return normal[a] < normal[b]; });
+        std::vector<uint32_t> inv(n), sn(n), ss(n);
+        std::vector<float> sc(n);
+        for (uint32_t k = 0; k < n; ++k) {
+            inv[perm[k]] = k;
+            sn[k] = normal[perm[k]]; ss[k] = shifted[perm[k]]; sc[k] = coeff[perm[k]];
+        }
+        e->h_mur_normal = sn;
+        e->h_mur_shifted = ss;
         std::unordered_map<uint32_t, uint32_t> last;
         std::vector<uint32_t> order;
         for (uint32_t i = 0; i < n; ++i) {
@@ -927,11 +941,13 @@ efs_status efs_configure_mur(efs_engine* e, const float* coeff, const uint32_t* 
             if (it == last.end()) { last.emplace(normal[i], i); order.push_back(normal[i]); }
             else it->second = i;
         }
+        std::sort(order.begin(), order.end());
         std::vector<uint32_t> at(order.size()), as(order.size());
-        for (size_t i = 0; i < order.size(); ++i) { at[i] = order[i]; as[i] = last[order[i]]; }
-        e->upload(e->mur_coeff, coeff, n);
-        e->upload(e->mur_shifted, shifted, n);
+        for (size_t i = 0; i < order.size(); ++i) { at[i] = order[i]; as[i] = inv[last[order[i]]]; }
+        e->upload(e->mur_coeff, sc);
+        e->upload(e->mur_shifted, ss);
         e->upload(e->mur_apply_target, at); e->upload(e->mur_apply_src, as);
+        e->mur_perm = perm;
         e->h_mur_apply = at;
         e->alloc(e->mur_saved, (size_t)n * 4);
         e->mur_n = n; e->mur_napply = (uint32_t)order.size();
@@ -1501,7 +1517,9 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
         std::vector<float> tmp(n);
         if (n) ck(cudaMemcpyAsync(tmp.data(), b->p, n * 4, cudaMemcpyDeviceToHost, e->stream), "debug read");
         e->sync("sync");
-        if (s.rfind("rlc_", 0) == 0) {
+        if (s == "mur_saved") {
+            for (size_t k = 0; k < n; ++k) out[e->mur_perm[k]] = tmp[k];   // caller's entry order
+        } else if (s.rfind("rlc_", 0) == 0) {
             // device keeps elements grouped by field cell; restore caller order
             const size_t w = (s == "rlc_vil") ? 1 : 3;
             for (size_t i = 0; i < e->rlc_n; ++i)
