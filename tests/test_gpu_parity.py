@@ -194,6 +194,38 @@ def test_mur_with_pml_corners_bitexact(cuda_engine_cls):
     assert_bitexact(g.debugRead("mur_saved"), o.read("mur_saved"), "mur_saved")
 
 
+@pytest.mark.parametrize("N", [(16, 18, 24), (16, 17, 24)])
+def test_mur_six_faces_with_sources_bitexact(cuda_engine_cls, N):
+    """Mur on all six faces (edge and corner cells carry two entries), an
+    excitation and TFSF points inside: on the TMA path the Mur post-update and
+    apply run inside the core kernel; Ny = 17 (a y tile would start on the
+    y-hi face) keeps them in their own kernels.  Both bit for bit."""
+    from efs_b200 import opgen
+    mesh = opgen.Mesh(*[opgen.uniform_lines(n, 1e-3) for n in N])
+    mur = opgen.mur_dual(mesh, 1.5e-12, [(a, s) for a in range(3) for s in ("lo", "hi")])
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 43))
+    sig = np.sin(np.arange(30) * 0.4).astype(np.float32)
+    exc = dict(signal=sig, delay=[0, 2], amp=[1.0, 0.5], dir=[2, 1], pos=[idx(0, 8, 9, 12, *N), idx(0, 5, 6, 7, *N)],
+               period=0)
+    t = 3 * N[0] * N[1] * N[2]
+    r = np.random.default_rng(44)
+    inner = [idx(int(r.integers(0, 3)), int(r.integers(3, N[0] - 3)), int(r.integers(3, N[1] - 3)),
+                 int(r.integers(3, N[2] - 3)), *N) for _ in range(20)]
+    vp = [dict(field_idx=f, delay_int=int(r.integers(0, 4)), delay_frac=float(r.random()), amp=float(r.standard_normal()))
+          for f in inner]
+    cp = [dict(field_idx=int(r.integers(0, t)), delay_int=1, delay_frac=0.5, amp=0.3) for _ in range(10)]
+    for e in (g, o):
+        e.configureMur(mur)
+        e.configureExcitation(exc)
+        e.configureTFSF(dict(signal=sig, period=0, voltagePoints=vp, currentPoints=cp))
+    seed_fields(g, o, N, 45)
+    for n in (1, 30):
+        g.iterate(n)
+        o.iterate(n)
+        compare_fields(g, o, "mur6 +%d" % n)
+        assert_bitexact(g.debugRead("mur_saved"), o.read("mur_saved"), "mur_saved")
+
+
 def test_tfsf_bitexact(cuda_engine_cls):
     N = (10, 11, 12)
     g, o = both(cuda_engine_cls, N, rand_coeffs(N, 16))
