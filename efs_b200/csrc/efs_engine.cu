@@ -147,6 +147,11 @@ struct efs_engine {
         std::vector<uint32_t> h_field;   // dir*N + pos
         DevBuf src, lorentz, kint, kext, klor, state, lor;
         uint32_t n = 0;
+        // A side whose coefficients are all zero keeps its state at +0 while
+        // the fields stay finite (0*x + 0*y rounds to +0), so its kernel is
+        // skipped until a restored state may have put other values there.
+        bool zero = false, clean = true;
+        bool live() const { return n && !(zero && clean); }
     };
     AdeSide ade_v, ade_c;
 
@@ -408,7 +413,7 @@ struct efs_engine {
         if (ss_on)
             k_steady_state<<<blocks(ss_n, T), T, 0, stream>>>(V, st, k, ss_idx.as<uint32_t>(), ss_n, ss_period,
                                                               ss_e1.as<float>(), ss_e2.as<float>());
-        if (ade_v.n) k_ade<<<blocks(ade_v.n, T), T, 0, stream>>>(V, ade_dev(ade_v, vfl));
+        if (ade_v.live()) k_ade<<<blocks(ade_v.n, T), T, 0, stream>>>(V, ade_dev(ade_v, vfl));
         MurDev md = mur_dev(vfl);
         if (mur_on) k_mur_pre<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
         RlcDev rd = rlc_dev();
@@ -417,7 +422,7 @@ struct efs_engine {
         if (fused) {
             // ADE(curr) reads H and the current flux, which the E side never
             // touches: it runs before the fused kernel overwrites the flux.
-            if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            if (ade_c.live()) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
             if (pml_split()) launch_pml_e(p);
             launch_fused(p);
             if (pml_split()) launch_pml_h(p);
@@ -446,7 +451,7 @@ struct efs_engine {
             }
         } else {
             // --- pre-current ---
-            if (ade_c.n) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            if (ade_c.live()) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
             // --- core H (+UPML) ---
             dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
             if (indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, stream>>>(g, ps); }
@@ -1013,6 +1018,8 @@ efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order*
                 }
             }
             s.n = (uint32_t)s.h_field.size();
+            s.zero = true;
+            for (size_t i = 0; i < ki.size() && s.zero; ++i) s.zero = ki[i] == 0.f && ke[i] == 0.f && kl[i] == 0.f;
             e->upload(s.lorentz, lor); e->upload(s.kint, ki); e->upload(s.kext, ke); e->upload(s.klor, kl);
             e->alloc(s.state, (size_t)s.n * 4); e->alloc(s.lor, (size_t)s.n * 4);
         }
@@ -1486,6 +1493,10 @@ efs_status efs_set_state(efs_engine* e, const void* buf, size_t size) {
         e->sync("sync");
         e->numTS = (uint32_t)hdr[2];
         e->sync_state_to_device();
+        if (e->ade_v.zero || e->ade_c.zero) {   // restored ADE state may be non-zero: run those sides again
+            e->ade_v.clean = e->ade_c.clean = false;
+            e->dirty();
+        }
     });
 }
 
@@ -1593,7 +1604,7 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
         if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
         e->build_plan();
         uint32_t k = e->fused ? 1 + (e->defer_n > 0) + 2 * e->pml_split() : 2;   // fused (+ deferred H, UPML passes) or E and H
-        k += e->ss_on + (e->ade_v.n > 0) + (e->ade_c.n > 0) + 3 * e->mur_on + 2 * e->rlc_on;
+        k += e->ss_on + e->ade_v.live() + e->ade_c.live() + 3 * e->mur_on + 2 * e->rlc_on;
         k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
         k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;
         k += e->nf_on + e->ring_on;

@@ -2,12 +2,14 @@
 
     python -m efs_b200.profile_case --n 256 --steps 4
     python -m efs_b200.profile_case --batch 64 --steps 4
+    python -m efs_b200.profile_case --dispersive --steps 4
 
 The first builds workloads.large_plain(n) (n^3 lines: same features as the
 headline benchmark), configures the CUDA engine and runs `steps` timesteps,
 printing the mean device time per timestep.  --batch N instead builds the
 first N stub filters of the batched sweep (workloads.stub_filters) and runs
-them as one batch.  Sized by --n / --batch so a profiler capture stays small.
+them as one batch; --dispersive runs workloads.dispersive() (800 x 800 x 400).
+Sized by --n / --batch so a profiler capture stays small.
 """
 import argparse
 import time
@@ -17,6 +19,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=0, help="run N stub filters as one batch instead")
+    ap.add_argument("--dispersive", action="store_true", help="run the 800 x 800 x 400 dispersive solve instead")
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--time-core", type=int, default=0, help="also time N launches of the core kernel(s) alone")
@@ -47,7 +50,13 @@ def main():
         for e in engines:
             e.destroy()
         return
-    job = workloads.large_plain(args.n)
+    if args.dispersive:
+        t = time.perf_counter()
+        job = workloads.dispersive()
+        print("dispersive job built in %.1f s: %d dispersive cells" % (time.perf_counter() - t, job["dispersive_cells"]),
+              flush=True)
+    else:
+        job = workloads.large_plain(args.n)
     eng = CudaEngine()
     if not eng.initGPU():
         raise SystemExit("no CUDA device")
@@ -58,9 +67,9 @@ def main():
     eng.iterate(args.steps)
     eng.sync()
     dt = (time.perf_counter() - t) / max(1, args.steps)
-    N = args.n ** 3
-    line = "n=%d steps=%d  %.3f ms/timestep  %.1f MCells/s  kernels/step=%d" % (
-        args.n, args.steps, dt * 1e3, N / dt / 1e6, eng.kernelsPerStep())
+    N = job["grid"][0] * job["grid"][1] * job["grid"][2]
+    line = "grid=%s steps=%d  %.3f ms/timestep  %.1f MCells/s  kernels/step=%d  device %.1f GB" % (
+        "x".join(map(str, job["grid"])), args.steps, dt * 1e3, N / dt / 1e6, eng.kernelsPerStep(), eng.deviceBytes() / 1e9)
     if args.time_core:
         ms = eng.timeCore(args.time_core)
         core = ms[0] + ms[1]

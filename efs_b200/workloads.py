@@ -241,6 +241,113 @@ def patch_antenna(steps=30000, end_db=-50.0, pml=8):
                                 period=0))
 
 
+def _upml_boxes(grid, W):
+    """Six non-overlapping UPML slabs, `W` lines thick, on all faces of `grid`."""
+    Nx, Ny, Nz = grid
+    return [((0, 0, 0), (W, Ny, Nz)), ((Nx - W, 0, 0), (W, Ny, Nz)),
+            ((W, 0, 0), (Nx - 2 * W, W, Nz)), ((W, Ny - W, 0), (Nx - 2 * W, W, Nz)),
+            ((W, W, 0), (Nx - 2 * W, Ny - 2 * W, W)), ((W, W, Nz - W), (Nx - 2 * W, Ny - 2 * W, W))]
+
+
+def _dispersive_chunk(args):
+    """Operator rows of x-planes [x0, x1) for dispersive (runs in a worker):
+    vacuum with UPML on all faces."""
+    grid, delta, dT, x0, x1, pml = args
+    mesh = opgen.Mesh(*[opgen.uniform_lines(n, delta) for n in grid])
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, bc=(0, 0, 0, 0, 0, 0), x0=x0, x1=x1)
+    opgen.upml_apply(mesh, dT, _upml_boxes(grid, pml), [opgen.pml_sigma(mesh, a, pml, pml) for a in range(3)],
+                     vv, vi, ii, iv, x0=x0, build=False)
+    m, mt = opgen.to_indexed(vv, vi, ii, iv)
+    return x0, x1, m, mt.table()
+
+
+def dispersive(grid=(800, 800, 400), delta=0.25e-3, seed=5, pml=8, cover=0.3, nfreq=5, steps=40000, tfsf_inset=20,
+               nf2ff_inset=10, angle_deg=30.0, chunk=16, workers=None):
+    """Plain dispersive solve: a uniform grid (800 x 800 x 400 lines, 0.25 mm),
+    `pml`-cell UPML on all faces, seeded spheres (numpy default_rng(seed),
+    radius 5-40 cells, smaller on small grids) covering `cover` of the cells,
+    each single-pole Drude (omega_p = 1.4e16 rad/s, gamma = 3e13 1/s) or
+    Lorentz (delta_eps = 2, omega_0 = 2 pi 15 GHz, delta = 2 pi 1 GHz), a TFSF
+    Gaussian plane wave (10 GHz +- 5 GHz) at `angle_deg` from +z in the xz
+    plane, NF2FF with `nfreq` frequencies.  The spheres carry ADE state only:
+    the reference updates the auxiliary voltages every step and never applies
+    them to E or H (webgpu-fdtd.mjs:405-454, :1129-1172), so the ADE
+    coefficients here are a plain single-pole discretisation whose values do
+    not reach the fields.  Only the voltage side has coefficients; the
+    current side is all zero."""
+    Nx, Ny, Nz = grid
+    N = Nx * Ny * Nz
+    mesh = opgen.Mesh(*[opgen.uniform_lines(n, delta) for n in grid])
+    dT = opgen.cfl_dt(mesh)
+    items = [(tuple(grid), delta, dT, x0, min(Nx, x0 + chunk), pml) for x0 in range(0, Nx, chunk)]
+    if workers is None:
+        workers = min(len(items), max(1, os.cpu_count() or 1), 32)
+    mt = opgen.MaterialTable()
+    mat = np.empty(N, np.uint32)
+    for x0, x1, m, tab in _parallel_map(_dispersive_chunk, items, workers):
+        mat[x0 * Ny * Nz:x1 * Ny * Nz] = mt.add(tab)[m]
+    table = mt.table()
+    regions = opgen.upml_apply(mesh, dT, _upml_boxes(grid, pml), [opgen.pml_sigma(mesh, a, pml, pml) for a in range(3)],
+                               build=True)
+    # spheres: label 1 = Drude, 2 = Lorentz; a later sphere never relabels a cell
+    rng = np.random.default_rng(seed)
+    label = np.zeros(grid, np.uint8)
+    covered = 0
+    rmax = min(40, min(grid) // 2 - 1)
+    while covered < cover * N:
+        r = int(rng.integers(min(5, rmax), rmax + 1))
+        c = [int(rng.integers(r, n - r)) for n in grid]
+        kind = 1 if rng.random() < 0.5 else 2
+        sl = tuple(slice(c[a] - r, c[a] + r + 1) for a in range(3))
+        ax = np.arange(-r, r + 1) ** 2
+        ball = (ax[:, None, None] + ax[None, :, None] + ax[None, None, :]) <= r * r
+        sub = label[sl]
+        new = ball & (sub == 0)
+        sub[new] = kind
+        covered += int(new.sum())
+    eps0 = opgen.EPS0
+    wp, gam = 1.4e16, 3e13
+    d_int = (1 - gam * dT / 2) / (1 + gam * dT / 2)
+    d_ext = eps0 * wp * wp * dT * delta / (1 + gam * dT / 2)
+    w0, dl, de = 2 * math.pi * 15e9, 2 * math.pi * 1e9, 2.0
+    l_int = (1 - dl * dT) / (1 + dl * dT)
+    l_ext = eps0 * de * w0 * w0 * dT * delta / (1 + dl * dT)
+    l_lor = w0 * w0 * dT * dT
+    orders = []
+    flat = label.reshape(-1)
+    for kind, has_lor in ((1, False), (2, True)):
+        cells = np.flatnonzero(flat == kind).astype(np.uint32)
+        n = len(cells)
+        dirs = []
+        for d in range(3):
+            e = dict(dir=d, pos_idx=cells, v_int_ADE=np.full(n, d_int if kind == 1 else l_int, np.float32),
+                     v_ext_ADE=np.full(n, d_ext if kind == 1 else l_ext, np.float32))
+            if has_lor:
+                e["v_Lor_ADE"] = np.full(n, l_lor, np.float32)
+            dirs.append(e)
+        orders.append(dict(numCells=n, hasLorentz=has_lor, directions=dirs))
+    del label, flat
+    f0, fc = 10e9, 5e9
+    sig = opgen.gauss_signal(f0, fc, dT, steps).astype(np.float32)
+    th = math.radians(angle_deg)
+
+    def coef_at(kind_, comp, f):
+        return table[mat[f], (3 if kind_ == "E" else 9) + comp].astype(np.float64)
+    lo = [tfsf_inset] * 3
+    hi = [n - 1 - tfsf_inset for n in grid]
+    vp, cp = opgen.tfsf_plane_wave(mesh, dT, lo, hi, (math.sin(th), 0.0, math.cos(th)),
+                                   (math.cos(th), 0.0, -math.sin(th)), coef_at, len(sig))
+    pts, meta, primal, dual = opgen.nf2ff_box(mesh, [nf2ff_inset] * 3, [n - 1 - nf2ff_inset for n in grid])
+    freqs = [f0 + fc * (k - (nfreq - 1) / 2) / max(1, nfreq - 1) for k in range(nfreq)]
+    return dict(name="dispersive", grid=list(grid), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+                coefficients=dict(mat=mat, table=table), pml=regions, ade=dict(orders=orders),
+                tfsf=dict(signal=sig, period=0, voltagePoints=vp, currentPoints=cp),
+                nf2ff=dict(surfaceIndices=pts.ravel(), numPoints=len(pts), omegas=[2 * math.pi * f for f in freqs],
+                           dT=dT, gridSize=list(grid), primalEdgeLens=primal, dualEdgeLens=dual, maxTS=steps,
+                           windowType=0),
+                nf2ff_meta=meta, nf2ff_freqs=freqs, dispersive_cells=covered)
+
+
 def _stub_filter_one(args):
     """Coefficients of one microstrip stub filter (runs in a worker)."""
     grid, delta, dT, sub, w, stub, xa, xb, yc = args

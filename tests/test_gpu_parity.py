@@ -487,3 +487,47 @@ def test_openems_cavity_fixture_on_gpu(cuda_engine_cls):
     v = workloads.run_probe_job(g, job)
     err = np.linalg.norm(v - ref) / np.linalg.norm(ref)
     assert err < 1e-4, err
+
+
+def test_dispersive_small_bitexact(cuda_engine_cls):
+    """The dispersive workload at a small size: UPML on all faces, Drude and
+    Lorentz ADE on the voltage side (the current side has all-zero
+    coefficients and its kernel is skipped), TFSF at 30 degrees, NF2FF with 5
+    frequencies."""
+    from efs_b200 import workloads
+    job = workloads.dispersive(grid=(48, 40, 32), pml=4, chunk=8, steps=200, tfsf_inset=8, nf2ff_inset=6, workers=1)
+    g = cuda_engine_cls()
+    assert g.initGPU()
+    o = OracleEngine(mode="f32")
+    workloads.configure(g, job)
+    workloads.configure(o, job)
+    for n in (1, 40):
+        g.iterate(n)
+        o.iterate(n)
+        compare_fields(g, o, "dispersive +%d" % n)
+    for name in ("ade_volt", "ade_volt_lor", "ade_curr", "ade_curr_lor"):
+        ref = np.concatenate([o.read(name, oi, d) for oi in range(2) for d in range(3)])
+        assert_bitexact(g.debugRead(name), ref, name)
+    assert np.abs(np.asarray(g.debugRead("ade_volt"))).max() > 0
+    ag, ao = g.readNF2FFAccumulation(True), o.readNF2FFAccumulation(True)
+    for k in ("accumE", "accumH"):
+        a, b = np.asarray(ag[k], np.float64), np.asarray(ao[k], np.float64)
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), k
+    # A restored state may hold non-zero values on the zero-coefficient side:
+    # the next step must run that side again, which sets them back to 0.
+    blob = bytearray(np.asarray(g.getState(), np.uint8).tobytes())
+    pos, nb = 32, []
+    while pos < len(blob):
+        n = int(np.frombuffer(blob, np.uint64, 1, pos)[0])
+        nb.append((pos + 8, n))
+        pos += 8 + n
+    off, n = nb[-4]                     # ..., ADE curr state, ADE curr lor, NF2FF E, NF2FF H
+    assert n == 4 * 3 * sum(od["numCells"] for od in job["ade"]["orders"])
+    blob[off:off + n] = np.ones(n // 4, np.float32).tobytes()
+    g.setState(np.frombuffer(bytes(blob), np.uint8))
+    assert np.all(np.asarray(g.debugRead("ade_curr")) == 1)
+    g.iterate(1)
+    o.iterate(1)
+    compare_fields(g, o, "dispersive after restore")
+    assert np.all(np.asarray(g.debugRead("ade_curr")).view(np.uint32) == 0)
+    g.destroy()
