@@ -116,6 +116,7 @@ struct efs_engine {
         uint32_t s[3], n[3];
         size_t total;
         DevBuf vv, vvfo, vvfn, ii, iifo, iifn, vflux, cflux, vflux_b, cflux_b;
+        DevBuf cidx, ctab;      // compact coefficients (empty when the region has too many distinct tuples)
         float* vf(int p) const { return (p && vflux_b.p) ? vflux_b.as<float>() : vflux.as<float>(); }
         float* cf(int p) const { return (p && cflux_b.p) ? cflux_b.as<float>() : cflux.as<float>(); }
     };
@@ -145,7 +146,8 @@ struct efs_engine {
     bool ade_on = false;
     struct AdeSide {
         std::vector<uint32_t> h_field;   // dir*N + pos
-        DevBuf src, lorentz, kint, kext, klor, state, lor;
+        std::vector<uint32_t> h_coef;    // per entry: coefficient tuple id, bit 31 set for Lorentz
+        DevBuf runs, quad_run, coef, state, lor;
         uint32_t n = 0;
         // A side whose coefficients are all zero keeps its state at +0 while
         // the fields stay finite (0*x + 0*y rounds to +0), so its kernel is
@@ -280,6 +282,8 @@ struct efs_engine {
             s.r[r].vv = R.vv.as<float>(); s.r[r].vvfo = R.vvfo.as<float>(); s.r[r].vvfn = R.vvfn.as<float>();
             s.r[r].ii = R.ii.as<float>(); s.r[r].iifo = R.iifo.as<float>(); s.r[r].iifn = R.iifn.as<float>();
             s.r[r].vflux = R.vf(p); s.r[r].cflux = R.cf(p);
+            s.r[r].cidx = R.cidx.p ? R.cidx.as<uint16_t>() : nullptr;
+            s.r[r].ctab = R.cidx.p ? R.ctab.as<float4>() : nullptr;
         }
         return s;
     }
@@ -324,9 +328,29 @@ struct efs_engine {
         }
         for (AdeSide* s : {&ade_v, &ade_c}) {
             if (!s->n) continue;
-            std::vector<ReadLoc> src(s->n);
-            for (uint32_t i = 0; i < s->n; ++i) src[i] = redirect(s->h_field[i]);
-            upload(s->src, src);
+            std::vector<AdeRun> runs;
+            ReadLoc prev{0, 0};
+            for (uint32_t i = 0; i < s->n; ++i) {
+                const ReadLoc l = redirect(s->h_field[i]);
+                const uint32_t c = s->h_coef[i];
+                if (i == 0 || l.sel != prev.sel || l.idx != prev.idx + 1 || c != runs.back().coef)
+                    runs.push_back(AdeRun{i, l.sel, l.idx, c});
+                prev = l;
+            }
+            if (runs.size() >= 0x80000000u) fail(EFS_ERR_INVALID, "too many ADE runs");
+            const uint32_t nq = (s->n + ADE_V - 1) / ADE_V;
+            std::vector<uint32_t> qr(nq);
+            size_t r = 0;
+            for (uint32_t q = 0; q < nq; ++q) {
+                const uint32_t i0 = q * ADE_V, i1 = std::min(s->n, i0 + ADE_V);
+                while (r + 1 < runs.size() && runs[r + 1].entry <= i0) ++r;
+                uint32_t lor = 0;
+                for (size_t k = r; k < runs.size() && runs[k].entry < i1; ++k) lor |= runs[k].coef & 0x80000000u;
+                qr[q] = (uint32_t)r | lor;
+            }
+            runs.push_back(AdeRun{s->n, 0, 0, 0});      // sentinel: ends the last run
+            upload(s->runs, runs);
+            upload(s->quad_run, qr);
         }
         plan_dirty = false;
     }
@@ -413,7 +437,7 @@ struct efs_engine {
         if (ss_on)
             k_steady_state<<<blocks(ss_n, T), T, 0, stream>>>(V, st, k, ss_idx.as<uint32_t>(), ss_n, ss_period,
                                                               ss_e1.as<float>(), ss_e2.as<float>());
-        if (ade_v.live()) k_ade<<<blocks(ade_v.n, T), T, 0, stream>>>(V, ade_dev(ade_v, vfl));
+        if (ade_v.live()) k_ade<<<blocks(ade_v.n, ADE_BLOCK), ADE_T, 0, stream>>>(V, ade_dev(ade_v, vfl));
         MurDev md = mur_dev(vfl);
         if (mur_on) k_mur_pre<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
         RlcDev rd = rlc_dev();
@@ -422,7 +446,7 @@ struct efs_engine {
         if (fused) {
             // ADE(curr) reads H and the current flux, which the E side never
             // touches: it runs before the fused kernel overwrites the flux.
-            if (ade_c.live()) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
             if (pml_split()) launch_pml_e(p);
             launch_fused(p);
             if (pml_split()) launch_pml_h(p);
@@ -451,7 +475,7 @@ struct efs_engine {
             }
         } else {
             // --- pre-current ---
-            if (ade_c.live()) k_ade<<<blocks(ade_c.n, T), T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+            if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
             // --- core H (+UPML) ---
             dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
             if (indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, stream>>>(g, ps); }
@@ -590,8 +614,8 @@ struct efs_engine {
                             p.amp.as<float>(), p.frac.as<float>(), sig.as<float>(), len, period};
     }
     AdeDev ade_dev(const AdeSide& s, const float* const* flux) const {
-        return AdeDev{s.n, s.src.as<ReadLoc>(), s.lorentz.as<uint8_t>(), s.kint.as<float>(), s.kext.as<float>(),
-                      s.klor.as<float>(), s.state.as<float>(), s.lor.as<float>(), flux};
+        return AdeDev{s.n, s.runs.as<AdeRun>(), s.quad_run.as<uint32_t>(), s.coef.as<float4>(), s.state.as<float>(),
+                      s.lor.as<float>(), flux};
     }
     MurDev mur_dev(const float* const* vfl) const {
         return MurDev{mur_n, mur_napply, mur_coeff.as<float>(), mur_pre_normal.as<ReadLoc>(), mur_pre_shifted.as<ReadLoc>(),
@@ -873,6 +897,48 @@ efs_status efs_configure_excitation(efs_engine* e, const float* signal, uint32_t
     });
 }
 
+// The distinct (vv, vvfo, vvfn, ii, iifo, iifn) x 3-component tuples of a
+// region's cells as a row table and a 16-bit row index per cell.  A UPML's
+// coefficients follow its grading profiles, so a slab has a few thousand
+// distinct tuples at most; a region with more keeps only the dense arrays.
+static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_region& in) {
+    const size_t nc = R.total / 3;
+    const float* src[6] = {in.vv, in.vvfo, in.vvfn, in.ii, in.iifo, in.iifn};
+    typedef std::array<uint32_t, 18> Key;
+    struct KeyHash {
+        size_t operator()(const Key& k) const {
+            uint64_t h = 1469598103934665603ull;
+            for (uint32_t v : k) { h ^= v; h *= 1099511628211ull; }
+            return (size_t)h;
+        }
+    };
+    std::unordered_map<Key, uint32_t, KeyHash> ids;
+    std::vector<uint16_t> idx(nc);
+    std::vector<float> tab;
+    Key key{}, last{};
+    uint32_t last_id = 0;
+    for (size_t c = 0; c < nc; ++c) {
+        for (int a = 0; a < 6; ++a)
+            for (int n = 0; n < 3; ++n) memcpy(&key[a * 3 + n], src[a] + n * nc + c, 4);
+        if (c == 0 || key != last) {
+            auto it = ids.find(key);
+            if (it == ids.end()) {
+                if (ids.size() >= 65535) { R.cidx.reset(); R.ctab.reset(); return; }
+                it = ids.emplace(key, (uint32_t)ids.size()).first;
+                for (int a = 0; a < 6; ++a) {
+                    for (int n = 0; n < 3; ++n) { float f; memcpy(&f, &key[a * 3 + n], 4); tab.push_back(f); }
+                    tab.push_back(0.f);
+                }
+            }
+            last = key;
+            last_id = it->second;
+        }
+        idx[c] = (uint16_t)last_id;
+    }
+    e->upload(R.cidx, idx);
+    e->upload(R.ctab, tab);
+}
+
 efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region* regions) {
     return guard(e, [&] {
         e->need_init();
@@ -892,6 +958,7 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
             R->total = 3 * (size_t)R->n[0] * R->n[1] * R->n[2];
             e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
             e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
+            compact_pml(e, *R, in);
             e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
             if (e->fused) { e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4); }
             out.push_back(std::move(R));
@@ -998,8 +1065,12 @@ efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order*
         for (int side = 0; side < 2; ++side) {
             efs_engine::AdeSide& s = side == 0 ? e->ade_v : e->ade_c;
             s = efs_engine::AdeSide();
-            std::vector<uint8_t> lor;
-            std::vector<float> ki, ke, kl;
+            // coefficient tuples (kint, kext, klor bits + Lorentz flag), deduplicated
+            std::map<std::array<uint32_t, 4>, uint32_t> ids;
+            std::vector<float4> tuples;
+            std::array<uint32_t, 4> last{};
+            uint32_t last_id = 0;
+            auto bits = [](float f) { uint32_t u; memcpy(&u, &f, 4); return u; };
             for (uint32_t o = 0; o < count; ++o) {
                 const efs_ade_order& od = orders[o];
                 if (od.num_directions && !od.directions) fail(EFS_ERR_INVALID, "ADE directions must be non-null");
@@ -1012,15 +1083,27 @@ efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order*
                     for (uint32_t i = 0; i < od.num_cells; ++i) {
                         if (dr.pos_idx[i] >= e->N) fail(EFS_ERR_INVALID, "ADE pos_idx out of range");
                         s.h_field.push_back(dr.dir * (uint32_t)e->N + dr.pos_idx[i]);
-                        lor.push_back(od.has_lorentz ? 1 : 0);
-                        ki.push_back(a ? a[i] : 0.f); ke.push_back(b ? b[i] : 0.f); kl.push_back(c ? c[i] : 0.f);
+                        const float k0 = a ? a[i] : 0.f, k1 = b ? b[i] : 0.f, k2 = c ? c[i] : 0.f;
+                        const std::array<uint32_t, 4> key{bits(k0), bits(k1), bits(k2), od.has_lorentz ? 1u : 0u};
+                        if (tuples.empty() || key != last) {
+                            auto it = ids.find(key);
+                            if (it == ids.end()) {
+                                if (tuples.size() >= 0x7fffffffu) fail(EFS_ERR_INVALID, "too many ADE coefficient tuples");
+                                it = ids.emplace(key, (uint32_t)tuples.size()).first;
+                                tuples.push_back(make_float4(k0, k1, k2, 0.f));
+                            }
+                            last = key;
+                            last_id = it->second | (key[3] << 31);
+                        }
+                        s.h_coef.push_back(last_id);
                     }
                 }
             }
             s.n = (uint32_t)s.h_field.size();
+            // all coefficients +0 (bit for bit: a -0 coefficient can make a -0 state)
             s.zero = true;
-            for (size_t i = 0; i < ki.size() && s.zero; ++i) s.zero = ki[i] == 0.f && ke[i] == 0.f && kl[i] == 0.f;
-            e->upload(s.lorentz, lor); e->upload(s.kint, ki); e->upload(s.kext, ke); e->upload(s.klor, kl);
+            for (const auto& kv : ids) s.zero = s.zero && !kv.first[0] && !kv.first[1] && !kv.first[2];
+            e->upload(s.coef, tuples);
             e->alloc(s.state, (size_t)s.n * 4); e->alloc(s.lor, (size_t)s.n * 4);
         }
         e->ade_on = count > 0;

@@ -28,6 +28,10 @@ struct PmlRegion {
     const float* vv; const float* vvfo; const float* vvfn;
     const float* ii; const float* iifo; const float* iifn;
     float* vflux; float* cflux;
+    // Optional compact form of the six coefficient arrays (null when a region
+    // has more than 65535 distinct cell tuples): per cell a row index, per row
+    // six float4 {vv, vvfo, vvfn, ii, iifo, iifn} x 3 components (+ pad).
+    const uint16_t* cidx; const float4* ctab;
 };
 struct PmlSet {
     int count;
@@ -336,26 +340,75 @@ __global__ void k_mur_post(const float* __restrict__ V, const MurDev m) { mur_po
 __global__ void k_mur_apply(float* __restrict__ V, const MurDev m) { mur_apply_body(V, m, blockIdx.x * blockDim.x + threadIdx.x); }
 
 // Lorentz/Drude ADE state update (src/webgpu-fdtd.mjs:405-454), all orders
-// and directions of one field flattened into one list.
+// and directions of one field flattened into one list of entries.  The
+// per-entry locations and coefficients are stored as runs: the entries
+// [run.entry, next run.entry) read consecutive locations from (sel, idx) on
+// and share one coefficient tuple, so a sphere row costs one 16-byte run
+// instead of 21 bytes per entry.  A thread updates the ADE_V consecutive
+// entries of one quad (state and Lorentz state as one 16-byte access each, so
+// enough bytes are in flight per SM).  quad_run[q] names the run of entry
+// q*ADE_V (bit 31: the quad holds a Lorentz entry), so the state, Lorentz
+// state and run loads issue together and the field load follows; the thread
+// steps forward across run starts inside its quad.  The run list ends with a
+// sentinel run whose entry is n.
+constexpr uint32_t ADE_T = 256;                 // threads per block
+constexpr uint32_t ADE_V = 4;                   // entries per thread (one quad)
+constexpr uint32_t ADE_BLOCK = ADE_T * ADE_V;   // entries per block
+struct AdeRun { uint32_t entry, sel, idx, coef; };   // coef: tuple id, bit 31 set for Lorentz
 struct AdeDev {
     uint32_t n;
-    const ReadLoc* src;
-    const uint8_t* lorentz;
-    const float* kint; const float* kext; const float* klor;
-    float* state; float* lor;
+    const AdeRun* runs;             // + sentinel {n, 0, 0, 0}
+    const uint32_t* quad_run;       // per quad: run of its first entry, bit 31 if it holds a Lorentz entry
+    const float4* coef;             // per tuple: kint, kext, klor, 0
+    float* state; float* lor;       // 16-byte aligned
     const float* const* flux;
 };
-__global__ void k_ade(const float* __restrict__ F, const AdeDev a) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const float v = read_loc(F, a.flux, a.src[i]);
-    const float st = a.state[i];
-    if (a.lorentz[i]) {
-        const float l = __fadd_rn(a.lor[i], __fmul_rn(a.klor[i], st));
-        a.lor[i] = l;
-        a.state[i] = __fadd_rn(__fmul_rn(a.kint[i], st), __fmul_rn(a.kext[i], __fsub_rn(v, l)));
+__device__ __forceinline__ float ade_one(float v, float st, float& l, uint32_t cid, const float4& c) {
+    if (cid >> 31) {
+        l = __fadd_rn(l, __fmul_rn(c.z, st));
+        return __fadd_rn(__fmul_rn(c.x, st), __fmul_rn(c.y, __fsub_rn(v, l)));
+    }
+    return __fadd_rn(__fmul_rn(c.x, st), __fmul_rn(c.y, v));
+}
+__global__ void __launch_bounds__(ADE_T) k_ade(const float* __restrict__ F, const AdeDev a) {
+    const uint32_t q = blockIdx.x * ADE_T + threadIdx.x, i0 = q * ADE_V;
+    if (i0 >= a.n) return;
+    const uint32_t cnt = min(ADE_V, a.n - i0);
+    const uint32_t qr = __ldg(a.quad_run + q);
+    float4 st = make_float4(0.f, 0.f, 0.f, 0.f), lr = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (cnt == ADE_V) {
+        st = *reinterpret_cast<const float4*>(a.state + i0);
+        if (qr >> 31) lr = *reinterpret_cast<const float4*>(a.lor + i0);
+    }
+    uint32_t lo = qr & 0x7fffffffu;
+    AdeRun r = a.runs[lo];
+    uint32_t next = a.runs[lo + 1].entry;
+    float v[ADE_V];
+    uint32_t cid[ADE_V];
+#pragma unroll
+    for (uint32_t k = 0; k < ADE_V; ++k) {
+        cid[k] = 0;
+        v[k] = 0.f;
+        if (k < cnt) {
+            const uint32_t i = i0 + k;
+            while (i >= next) { ++lo; r = a.runs[lo]; next = a.runs[lo + 1].entry; }
+            v[k] = read_loc(F, a.flux, ReadLoc{r.sel, r.idx + (i - r.entry)});
+            cid[k] = r.coef;
+        }
+    }
+    if (cnt == ADE_V) {
+        st.x = ade_one(v[0], st.x, lr.x, cid[0], a.coef[cid[0] & 0x7fffffffu]);
+        st.y = ade_one(v[1], st.y, lr.y, cid[1], a.coef[cid[1] & 0x7fffffffu]);
+        st.z = ade_one(v[2], st.z, lr.z, cid[2], a.coef[cid[2] & 0x7fffffffu]);
+        st.w = ade_one(v[3], st.w, lr.w, cid[3], a.coef[cid[3] & 0x7fffffffu]);
+        *reinterpret_cast<float4*>(a.state + i0) = st;
+        if (qr >> 31) *reinterpret_cast<float4*>(a.lor + i0) = lr;
     } else {
-        a.state[i] = __fadd_rn(__fmul_rn(a.kint[i], st), __fmul_rn(a.kext[i], v));
+        for (uint32_t k = 0; k < cnt; ++k) {
+            float l = a.lor[i0 + k];
+            a.state[i0 + k] = ade_one(v[k], a.state[i0 + k], l, cid[k], a.coef[cid[k] & 0x7fffffffu]);
+            if (cid[k] >> 31) a.lor[i0 + k] = l;
+        }
     }
 }
 

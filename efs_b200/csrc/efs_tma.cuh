@@ -357,12 +357,21 @@ k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUt
 // chain over all of them in region order.
 //
 // Both passes are latency-bound (a z-slab region row is 8 cells, 32 bytes,
-// long), so a thread takes PML_ZC consecutive z cells of one region row and
+// long).  A thread takes PML_ZC consecutive z cells of one region row and
 // issues every load of them (fields, material index and, for the usual
-// single-region cell, the region's coefficients and flux) before any
-// arithmetic.
+// single-region cell, the region's flux and compact coefficient row) before
+// any arithmetic.  Measured on B200 over PML_ZC in {1, 2, 4} x {2, 3, 4, 6}
+// blocks per SM, one cell per thread at 4 blocks per SM (64 registers, no
+// spills) is fastest: occupancy hides more latency than per-thread batching.
 // ---------------------------------------------------------------------------
-constexpr uint32_t PML_ZC = 2;
+#ifndef EFS_PML_ZC
+#define EFS_PML_ZC 1
+#endif
+#ifndef EFS_PML_MINB
+#define EFS_PML_MINB 4
+#endif
+constexpr uint32_t PML_ZC = EFS_PML_ZC;     // z cells per thread
+constexpr int PML_MINB = EFS_PML_MINB;      // resident 256-thread blocks per SM the register budget is set for
 
 // Work item i -> region r, row (x, y), first z and cell count (PML_ZC cells
 // per item along z, items in region order).
@@ -396,17 +405,28 @@ __device__ __forceinline__ uint32_t pml_owner_mask(const PmlSet& ps, int r, uint
 }
 
 // Region coefficients and old flux of one single-region cell (3 components).
+// With the compact form the three coefficients come from one table row
+// (three float4 loads that hit L1/L2) instead of nine per-cell loads.
 template <bool VOLT>
 __device__ __forceinline__ void pml_fetch(const PmlRegion& R, uint32_t x, uint32_t y, uint32_t z, float a[3], float b[3],
                                           float fn[3], float fo[3]) {
     const size_t p0 = region_p(R, 0, x, y, z), nreg = (size_t)R.n[0] * R.n[1] * R.n[2];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) fo[n] = __ldg((VOLT ? R.vflux : R.cflux) + p0 + n * nreg);
+    if (R.cidx) {
+        const float4* row = R.ctab + 6 * (uint32_t)__ldg(R.cidx + p0) + (VOLT ? 0 : 3);
+        const float4 ka = __ldg(row), kb = __ldg(row + 1), kf = __ldg(row + 2);
+        a[0] = ka.x; a[1] = ka.y; a[2] = ka.z;
+        b[0] = kb.x; b[1] = kb.y; b[2] = kb.z;
+        fn[0] = kf.x; fn[1] = kf.y; fn[2] = kf.z;
+        return;
+    }
 #pragma unroll
     for (int n = 0; n < 3; ++n) {
         const size_t p = p0 + n * nreg;
         a[n] = __ldg((VOLT ? R.vv : R.ii) + p);
         b[n] = __ldg((VOLT ? R.vvfo : R.iifo) + p);
         fn[n] = __ldg((VOLT ? R.vvfn : R.iifn) + p);
-        fo[n] = __ldg((VOLT ? R.vflux : R.cflux) + p);
     }
 }
 
@@ -480,7 +500,7 @@ __device__ __forceinline__ void pml_e_body(const FusedGrid& g, const PmlSet& ps,
     }
 }
 template <bool IDX>
-__global__ void __launch_bounds__(256) k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t items) {
+__global__ void __launch_bounds__(256, PML_MINB) k_pml_e(const FusedGrid g, const PmlSet ps, const PmlSet pn, float* V0w, uint32_t items) {
     pml_e_body<IDX>(g, ps, pn, V0w, items, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -547,7 +567,7 @@ __device__ __forceinline__ void pml_h_body(const FusedGrid& g, const PmlSet& ps,
     }
 }
 template <bool IDX>
-__global__ void __launch_bounds__(256) k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t items) {
+__global__ void __launch_bounds__(256, PML_MINB) k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t items) {
     pml_h_body<IDX>(g, ps, pn, items, blockIdx.x * blockDim.x + threadIdx.x);
 }
 

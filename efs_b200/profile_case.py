@@ -8,7 +8,8 @@ The first builds workloads.large_plain(n) (n^3 lines: same features as the
 headline benchmark), configures the CUDA engine and runs `steps` timesteps,
 printing the mean device time per timestep.  --batch N instead builds the
 first N stub filters of the batched sweep (workloads.stub_filters) and runs
-them as one batch; --dispersive runs workloads.dispersive() (800 x 800 x 400).
+them as one batch; --dispersive runs workloads.dispersive() (800 x 800 x 400,
+or --grid).
 Sized by --n / --batch so a profiler capture stays small.
 """
 import argparse
@@ -20,6 +21,7 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=0, help="run N stub filters as one batch instead")
     ap.add_argument("--dispersive", action="store_true", help="run the 800 x 800 x 400 dispersive solve instead")
+    ap.add_argument("--grid", type=int, nargs=3, default=[800, 800, 400], help="grid of the dispersive solve")
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--time-core", type=int, default=0, help="also time N launches of the core kernel(s) alone")
@@ -52,7 +54,7 @@ def main():
         return
     if args.dispersive:
         t = time.perf_counter()
-        job = workloads.dispersive()
+        job = workloads.dispersive(grid=tuple(args.grid))
         print("dispersive job built in %.1f s: %d dispersive cells" % (time.perf_counter() - t, job["dispersive_cells"]),
               flush=True)
     else:
