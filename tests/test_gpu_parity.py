@@ -243,6 +243,40 @@ def test_tfsf_bitexact(cuda_engine_cls):
     compare_fields(g, o, "tfsf")
 
 
+def test_tfsf_on_tile_seams_bitexact(cuda_engine_cls):
+    """TFSF targets on the seams of the core kernel's 64 x 8 (z x y) tiles
+    (halo rows, halo columns and their corners), on every x plane (x-chunk
+    seams in the small-chunk variants) and inside UPML regions, with repeated
+    targets: the H cells next to them are redone after the TFSF pass."""
+    N = (13, 20, 136)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 40))
+    regs = [pml_region((0, 0, 120), (13, 20, 16), 41), pml_region((0, 14, 0), (13, 6, 120), 42)]
+    for e in (g, o):
+        e.configurePML(regs)
+    r = np.random.default_rng(43)
+    ys, zs = [0, 7, 8, 15, 16, 19], [0, 1, 63, 64, 65, 127, 128, 135]
+
+    def pt(seam):
+        x = int(r.integers(0, N[0]))
+        y = int(r.choice(ys)) if seam else int(r.integers(0, N[1]))
+        z = int(r.choice(zs)) if seam else int(r.integers(0, N[2]))
+        return dict(field_idx=idx(int(r.integers(0, 3)), x, y, z, *N), delay_int=int(r.integers(0, 8)),
+                    delay_frac=float(r.random()), amp=float(r.standard_normal()))
+    vp = [pt(True) for _ in range(400)] + [pt(False) for _ in range(100)]
+    vp += [dict(vp[i]) for i in range(0, 400, 7)]          # repeated targets, applied in order
+    cp = [pt(True) for _ in range(150)]
+    cfg = dict(signal=np.sin(np.arange(50) * 0.3).astype(np.float32), period=0, voltagePoints=vp, currentPoints=cp)
+    for e in (g, o):
+        e.configureTFSF(cfg)
+    seed_fields(g, o, N, 44)
+    for n in (1, 6, 30):
+        g.iterate(n)
+        o.iterate(n)
+        compare_fields(g, o, "tfsf seams +%d" % n)
+    for k in range(len(regs)):
+        assert_bitexact(g.debugRead("pml_curr_flux", k), o.read("pml_curr_flux", k), "cflux %d" % k)
+
+
 def test_ade_in_and_out_of_pml_bitexact(cuda_engine_cls):
     N = (12, 10, 16)
     g, o = both(cuda_engine_cls, N, rand_coeffs(N, 18))
