@@ -147,7 +147,7 @@ struct efs_engine {
     struct AdeSide {
         std::vector<uint32_t> h_field;   // dir*N + pos
         std::vector<uint32_t> h_coef;    // per entry: coefficient tuple id, bit 31 set for Lorentz
-        DevBuf runs, quad_run, coef, state, lor;
+        DevBuf runs, grp_run, coef, state, lor;
         uint32_t n = 0;
         // A side whose coefficients are all zero keeps its state at +0 while
         // the fields stay finite (0*x + 0*y rounds to +0), so its kernel is
@@ -338,7 +338,7 @@ struct efs_engine {
                 prev = l;
             }
             if (runs.size() >= 0x80000000u) fail(EFS_ERR_INVALID, "too many ADE runs");
-            const uint32_t nq = (s->n + ADE_V - 1) / ADE_V;
+            const uint32_t nq = (s->n + ADE_V - 1) / ADE_V;   // groups of ADE_V entries
             std::vector<uint32_t> qr(nq);
             size_t r = 0;
             for (uint32_t q = 0; q < nq; ++q) {
@@ -350,7 +350,7 @@ struct efs_engine {
             }
             runs.push_back(AdeRun{s->n, 0, 0, 0});      // sentinel: ends the last run
             upload(s->runs, runs);
-            upload(s->quad_run, qr);
+            upload(s->grp_run, qr);
         }
         plan_dirty = false;
     }
@@ -614,7 +614,7 @@ struct efs_engine {
                             p.amp.as<float>(), p.frac.as<float>(), sig.as<float>(), len, period};
     }
     AdeDev ade_dev(const AdeSide& s, const float* const* flux) const {
-        return AdeDev{s.n, s.runs.as<AdeRun>(), s.quad_run.as<uint32_t>(), s.coef.as<float4>(), s.state.as<float>(),
+        return AdeDev{s.n, s.runs.as<AdeRun>(), s.grp_run.as<uint32_t>(), s.coef.as<float4>(), s.state.as<float>(),
                       s.lor.as<float>(), flux};
     }
     MurDev mur_dev(const float* const* vfl) const {

@@ -159,6 +159,23 @@ def test_pml_bitexact(cuda_engine_cls, overlap):
         assert_bitexact(g.debugRead("pml_curr_flux", r), o.read("pml_curr_flux", r), "cflux %d" % r)
 
 
+def test_pml_dense_coefficients_bitexact(cuda_engine_cls):
+    """A UPML region with more distinct coefficient tuples than the compact
+    form holds (65,535) keeps its dense arrays; next to a compact region."""
+    N = (40, 41, 48)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 50))
+    regs = [pml_region((0, 0, 0), (40, 41, 41), 51), pml_region((0, 0, 41), (40, 41, 7), 52)]
+    for e in (g, o):
+        e.configurePML(regs)
+    seed_fields(g, o, N, 53)
+    g.iterate(9)
+    o.iterate(9)
+    compare_fields(g, o, "pml dense")
+    for r in range(len(regs)):
+        assert_bitexact(g.debugRead("pml_volt_flux", r), o.read("pml_volt_flux", r), "vflux %d" % r)
+        assert_bitexact(g.debugRead("pml_curr_flux", r), o.read("pml_curr_flux", r), "cflux %d" % r)
+
+
 def mur_faces(N, coeff_seed):
     """Dual-component Mur on the x and y faces, with coinciding normals at the corners."""
     Nx, Ny, Nz = N
