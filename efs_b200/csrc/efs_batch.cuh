@@ -10,7 +10,7 @@
 //     tile origin, x-chunk) and runs each tile through the same TMA plane
 //     pipeline as the single engine, reading the member's grid, UPML set and
 //     tensor maps from a descriptor in global memory;
-//   * each sparse phase (Mur, excitation, TFSF, UPML passes, deferred H,
+//   * each sparse phase (Mur, excitation, TFSF, ADE, UPML passes, deferred H,
 //     NF2FF, probe ring, step counter) is one segmented launch: block b
 //     belongs to member seg[b] and runs the single engine's thread body on
 //     that member's arguments.
@@ -78,6 +78,10 @@ struct OpPoints {
     __device__ void run(uint32_t blk, uint32_t k, uint32_t, uint32_t) const {
         point_sources_body<KIND>(F, st, k, s, blk * blockDim.x + threadIdx.x);
     }
+};
+struct OpAde {
+    const float* F; AdeDev a;
+    __device__ void run(uint32_t blk, uint32_t, uint32_t, uint32_t) const { ade_body(F, a, blk * blockDim.x + threadIdx.x); }
 };
 struct OpRing {
     const float* V; const float* C; const StepState* st; RingDev r;
@@ -154,7 +158,7 @@ struct efs_batch {
     uint32_t phase = 0;
     DevBuf members[2], tiles[2];               // tiles[1]: material-index members, tiles[0]: dense members
     uint32_t ntiles[2] = {0, 0};
-    SegLaunch mur_pre[2], mur_post[2], mur_apply[2], exc[2], tfsf_v[2], tfsf_c[2], ring[2], nf_sample[2], nf_flush[2],
+    SegLaunch mur_pre[2], mur_post[2], mur_apply[2], exc[2], tfsf_v[2], tfsf_c[2], ade_v[2], ade_c[2], ring[2], nf_sample[2], nf_flush[2],
         deferred_i[2], deferred_d[2], pml_e_i[2], pml_e_d[2], pml_h_i[2], pml_h_d[2], advance;   // _i / _d: index / dense members
     bool any_nf = false;
     std::map<uint32_t, cudaGraphExec_t> graphs;
@@ -204,9 +208,9 @@ struct efs_batch {
             if (e->device != device) fail(EFS_ERR_INVALID, "batch members must share one device");
             if (!e->tma_path())
                 fail(EFS_ERR_STATE, "batch members need the TMA-fed fused path (Nz % 4 == 0, EFS_CORE / EFS_FUSED unset)");
-            if (e->ss_on || e->ade_v.n || e->ade_c.n || e->rlc_on || e->pbc_on)
-                fail(EFS_ERR_STATE, "batched stepping supports excitation, Mur, TFSF, UPML, NF2FF and the probe ring "
-                                    "(not steady state, ADE, RLC or PBC)");
+            if (e->ss_on || e->rlc_on || e->pbc_on)
+                fail(EFS_ERR_STATE, "batched stepping supports excitation, Mur, TFSF, ADE, UPML, NF2FF and the probe ring "
+                                    "(not steady state, RLC or PBC)");
         }
     }
 
@@ -225,6 +229,7 @@ struct efs_batch {
             std::vector<std::pair<uint32_t, OpMurApply>> mapply;
             std::vector<std::pair<uint32_t, OpPoints<0>>> vexc;
             std::vector<std::pair<uint32_t, OpPoints<1>>> vtv, vtc;
+            std::vector<std::pair<uint32_t, OpAde>> vav, vac;
             std::vector<std::pair<uint32_t, OpRing>> vring;
             std::vector<std::pair<uint32_t, OpNfSample>> vns;
             std::vector<std::pair<uint32_t, OpNfFlush>> vnf;
@@ -269,6 +274,11 @@ struct efs_batch {
                     vtv.push_back({e->tfsf_v.groups, OpPoints<1>{V1, st, e->point_dev(e->tfsf_v, e->tfsf_signal, e->tfsf_len, e->tfsf_period)}});
                 if (e->tfsf_on && e->tfsf_c.groups)
                     vtc.push_back({e->tfsf_c.groups, OpPoints<1>{C1, st, e->point_dev(e->tfsf_c, e->tfsf_signal, e->tfsf_len, e->tfsf_period)}});
+                // ADE: one thread per group of ADE_V entries; reads the pre-update fields and the old flux
+                if (e->ade_v.live())
+                    vav.push_back({(e->ade_v.n + ADE_V - 1) / ADE_V, OpAde{V, e->ade_dev(e->ade_v, e->vflux_ptrs[p].as<const float*>())}});
+                if (e->ade_c.live())
+                    vac.push_back({(e->ade_c.n + ADE_V - 1) / ADE_V, OpAde{e->cbuf(p), e->ade_dev(e->ade_c, e->cflux_ptrs[p].as<const float*>())}});
                 if (e->ring_on) vring.push_back({e->ring_n, OpRing{V1, C1, st, e->ring_dev()}});
                 if (e->nf_on) {
                     vns.push_back({e->nf.np, OpNfSample{V1, C1, e->nf}});
@@ -297,6 +307,8 @@ struct efs_batch {
             build_seg(exc[s], vexc);
             build_seg(tfsf_v[s], vtv);
             build_seg(tfsf_c[s], vtc);
+            build_seg(ade_v[s], vav);
+            build_seg(ade_c[s], vac);
             build_seg(ring[s], vring);
             build_seg(nf_sample[s], vns);
             build_seg(nf_flush[s], vnf);
@@ -331,7 +343,9 @@ struct efs_batch {
 
     // Timestep k of a captured batch at step phase s: the single engine's phase order, each phase for all members.
     void enqueue_step(uint32_t k, int s, bool last) {
+        launch_seg<OpAde>(ade_v[s], k);          // pre-voltage, as the single engine: ADE(volt), Mur pre
         launch_seg<OpMurPre>(mur_pre[s], k);
+        launch_seg<OpAde>(ade_c[s], k);          // ADE(curr) before the core update rewrites H and the flux
         launch_seg<OpPmlE<true>>(pml_e_i[s], k);
         launch_seg<OpPmlE<false>>(pml_e_d[s], k);
         const BatchMember* bm = members[s].as<BatchMember>();

@@ -371,9 +371,10 @@ __device__ __forceinline__ float ade_one(float v, float st, float& l, uint32_t c
     }
     return __fadd_rn(__fmul_rn(c.x, st), __fmul_rn(c.y, v));
 }
-__global__ void __launch_bounds__(ADE_T) k_ade(const float* __restrict__ F, const AdeDev a) {
+// Group q of one side (thread body shared with the batched form's segmented launch).
+__device__ __forceinline__ void ade_body(const float* __restrict__ F, const AdeDev& a, uint32_t q) {
     constexpr uint32_t NQ = ADE_V / 4;
-    const uint32_t q = blockIdx.x * ADE_T + threadIdx.x, i0 = q * ADE_V;
+    const uint32_t i0 = q * ADE_V;
     if (i0 >= a.n) return;
     const uint32_t cnt = min(ADE_V, a.n - i0);
     const uint32_t qr = __ldg(a.grp_run + q);
@@ -421,6 +422,9 @@ __global__ void __launch_bounds__(ADE_T) k_ade(const float* __restrict__ F, cons
             if (cid[k] >> 31) a.lor[i0 + k] = l;
         }
     }
+}
+__global__ void __launch_bounds__(ADE_T) k_ade(const float* __restrict__ F, const AdeDev a) {
+    ade_body(F, a, blockIdx.x * ADE_T + threadIdx.x);
 }
 
 // Lumped RLC (src/webgpu-fdtd.mjs:775-863, CPU order: pre before the core E

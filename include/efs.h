@@ -287,8 +287,8 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out);
  * and keeps its own step counter; between batch calls each member stays
  * usable through the per-engine calls (probe reads, energy, fields).  Members
  * need the TMA-fed fused path (Nz a multiple of 4) and may use excitation,
- * Mur, TFSF, UPML, NF2FF and the probe ring (not steady state, ADE, RLC,
- * PBC); members may mix material-index and dense coefficients.  Stepping
+ * Mur, TFSF, Lorentz/Drude ADE, UPML, NF2FF and the probe ring (not steady
+ * state, RLC, PBC); members may mix material-index and dense coefficients.  Stepping
  * or reconfiguring a member on its own between batch calls is allowed: the
  * batch re-plans. */
 typedef struct efs_batch efs_batch;

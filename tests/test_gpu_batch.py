@@ -1,9 +1,9 @@
 """Batched form (efs_batch_*) against the same engines stepped alone.
 
 Every member of a batch runs the single engine's thread bodies in the single
-engine's phase order, so its fields, probe ring, UPML fluxes and NF2FF
-accumulators must equal, bit for bit, those of an identical engine advanced
-on its own.  Members differ in grid size and extensions; batch calls use
+engine's phase order, so its fields, probe ring, UPML fluxes, ADE state and
+NF2FF accumulators must equal, bit for bit, those of an identical engine
+advanced on its own.  Members differ in grid size and extensions; batch calls use
 irregular step counts (one spans two captured graphs) and shapes.
 """
 import numpy as np
@@ -53,6 +53,15 @@ def member(cls, kind, indexed):
         g.configureTFSF(dict(signal=np.cos(np.arange(40) * 0.4).astype(np.float32), period=0, voltagePoints=vp,
                              currentPoints=cp))
         g.configureNF2FFAccumulation(nf2ff_inputs(N, nfreq=2, inset=5))
+    elif kind == 3:                       # dispersive: UPML on all faces, Drude/Lorentz ADE, oblique TFSF, NF2FF
+        from efs_b200 import opgen, workloads
+        job = workloads.dispersive(grid=(24, 20, 24), pml=3, chunk=8, steps=200, tfsf_inset=6, nf2ff_inset=4, workers=1)
+        N = tuple(job["grid"])
+        if not indexed:
+            vv, vi, ii, iv = opgen.dense_from_indexed(job["coefficients"]["mat"], job["coefficients"]["table"])
+            job = dict(job, coefficients=dict(vv=vv, vi=vi, ii=ii, iv=iv))
+        from efs_b200.workloads import configure
+        configure(g, job)
     else:                                 # small grid, excitation only
         N = (9, 11, 8)
         g.init(N, coeffs(N, 7, indexed))
@@ -74,6 +83,12 @@ def compare(a, b, kind, what):
         if ra is not None:
             assert ra["numSamples"] == rb["numSamples"]
             assert_bitexact(ra["data"], rb["data"], "ring")
+    if kind == 3:
+        for name in ("ade_volt", "ade_volt_lor", "ade_curr", "ade_curr_lor"):
+            assert_bitexact(a.debugRead(name), b.debugRead(name), "%s member 3 %s" % (what, name))
+        na, nb = a.readNF2FFAccumulation(True), b.readNF2FFAccumulation(True)
+        assert_bitexact(na["accumE"], nb["accumE"], "nf2ff E")
+        assert_bitexact(na["accumH"], nb["accumH"], "nf2ff H")
     if kind == 1:
         for r in range(3):
             assert_bitexact(a.debugRead("pml_volt_flux", r), b.debugRead("pml_volt_flux", r), "vflux")
@@ -86,7 +101,7 @@ def compare(a, b, kind, what):
 @pytest.mark.parametrize("indexed", [True, False])
 def test_batch_members_match_solo_engines(cuda_engine_cls, indexed):
     from efs_b200.engine import CudaBatch
-    kinds = (0, 1, 2)
+    kinds = (0, 1, 2, 3)
     batched = [member(cuda_engine_cls, k, indexed) for k in kinds]
     solo = [member(cuda_engine_cls, k, indexed) for k in kinds]
     b = CudaBatch(batched)
