@@ -245,6 +245,25 @@ struct efs_engine {
     }
 
     void need_init() const { if (!inited) fail(EFS_ERR_STATE, "engine not initialised: call efs_init first"); }
+    // Stable LSD radix sort of (key, value) pairs by key (8-bit digits; digits
+    // above the largest key are skipped).
+    static void radix_sort_pairs(std::vector<uint32_t>& key, std::vector<uint32_t>& val) {
+        const size_t n = key.size();
+        uint32_t kmax = 0;
+        for (uint32_t k : key) kmax = std::max(kmax, k);
+        std::vector<uint32_t> k2(n), v2(n);
+        for (int shift = 0; shift < 32 && (shift == 0 || (kmax >> shift) != 0); shift += 8) {
+            size_t cnt[257] = {0};
+            for (size_t i = 0; i < n; ++i) ++cnt[((key[i] >> shift) & 255u) + 1];
+            for (int d = 0; d < 256; ++d) cnt[d + 1] += cnt[d];
+            for (size_t i = 0; i < n; ++i) {
+                const size_t o = cnt[(key[i] >> shift) & 255u]++;
+                k2[o] = key[i]; v2[o] = val[i];
+            }
+            key.swap(k2); val.swap(v2);
+        }
+    }
+
     void check_idx3(const uint32_t* p, size_t n, const char* what) const {
         for (size_t i = 0; i < n; ++i)
             if (p[i] >= 3 * N) fail(EFS_ERR_INVALID, std::string(what) + ": index out of range");
@@ -687,17 +706,24 @@ struct efs_engine {
     }
 
     // group entries by target preserving order: returns unique targets + CSR offsets + permutation
+    // Entries grouped by target: utarget ascending, group g = entries
+    // perm[off[g] .. off[g+1]) in the caller's order (a stable sort by target).
     static void group_by(const std::vector<uint32_t>& tgt, std::vector<uint32_t>& utarget, std::vector<uint32_t>& off,
                          std::vector<uint32_t>& perm) {
-        std::unordered_map<uint32_t, uint32_t> first;
-        std::vector<std::vector<uint32_t>> lists;
-        for (uint32_t i = 0; i < tgt.size(); ++i) {
-            auto it = first.find(tgt[i]);
-            if (it == first.end()) { first.emplace(tgt[i], (uint32_t)lists.size()); lists.push_back({i}); utarget.push_back(tgt[i]); }
-            else lists[it->second].push_back(i);
-        }
+        const uint32_t n = (uint32_t)tgt.size();
+        std::vector<uint32_t> key(tgt);
+        perm.resize(n);
+        for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+        radix_sort_pairs(key, perm);
+        utarget.clear();
         off.assign(1, 0);
-        for (auto& l : lists) { for (uint32_t i : l) perm.push_back(i); off.push_back((uint32_t)perm.size()); }
+        for (uint32_t i = 0; i < n; ++i) {
+            if (i == 0 || key[i] != key[i - 1]) {
+                if (i) off.push_back(i);
+                utarget.push_back(key[i]);
+            }
+        }
+        if (n) off.push_back(n);
     }
 };
 
@@ -915,12 +941,23 @@ static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_regi
     std::unordered_map<Key, uint32_t, KeyHash> ids;
     std::vector<uint16_t> idx(nc);
     std::vector<float> tab;
+    // Lookups skip the map when the tuple equals the previous cell's (grading
+    // along x or y: constant along a z row) or the previous row's at the same
+    // z (grading along z: a z-slab row repeats its tuples).
+    const uint32_t nz = R.n[2];
+    std::vector<Key> zkey(nz);
+    std::vector<uint32_t> zid(nz);
     Key key{}, last{};
     uint32_t last_id = 0;
     for (size_t c = 0; c < nc; ++c) {
         for (int a = 0; a < 6; ++a)
             for (int n = 0; n < 3; ++n) memcpy(&key[a * 3 + n], src[a] + n * nc + c, 4);
-        if (c == 0 || key != last) {
+        const uint32_t z = (uint32_t)(c % nz);
+        if (c > 0 && key == last) {
+        } else if (c >= nz && key == zkey[z]) {
+            last = key;
+            last_id = zid[z];
+        } else {
             auto it = ids.find(key);
             if (it == ids.end()) {
                 if (ids.size() >= 65535) { R.cidx.reset(); R.ctab.reset(); return; }
@@ -933,6 +970,8 @@ static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_regi
             last = key;
             last_id = it->second;
         }
+        zkey[z] = key;
+        zid[z] = last_id;
         idx[c] = (uint16_t)last_id;
     }
     e->upload(R.cidx, idx);
@@ -995,34 +1034,26 @@ efs_status efs_configure_mur(efs_engine* e, const float* coeff, const uint32_t* 
         // face across rows).  The pre and post updates are per entry; apply
         // resolves each target to its last writer in the caller's order
         // (sequential loop :1016-1023), which the permutation leaves intact.
-        std::vector<uint32_t> perm(n);
+        std::vector<uint32_t> perm(n), sn(normal, normal + n);
         for (uint32_t i = 0; i < n; ++i) perm[i] = i;
-        std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) { return normal[a] < normal[b]; });
-        std::vector<uint32_t> inv(n), sn(n), ss(n);
+        efs_engine::radix_sort_pairs(sn, perm);           // stable: equal normals keep the caller's order
+        std::vector<uint32_t> ss(n);
         std::vector<float> sc(n);
-        for (uint32_t k = 0; k < n; ++k) {
-            inv[perm[k]] = k;
-            sn[k] = normal[perm[k]]; ss[k] = shifted[perm[k]]; sc[k] = coeff[perm[k]];
-        }
+        for (uint32_t k = 0; k < n; ++k) { ss[k] = shifted[perm[k]]; sc[k] = coeff[perm[k]]; }
+        // apply: per distinct normal (ascending) its last writer in the caller's
+        // order, which is the last entry of its run in the sorted order
+        std::vector<uint32_t> at, as;
+        for (uint32_t k = 0; k < n; ++k)
+            if (k + 1 == n || sn[k + 1] != sn[k]) { at.push_back(sn[k]); as.push_back(k); }
         e->h_mur_normal = sn;
         e->h_mur_shifted = ss;
-        std::unordered_map<uint32_t, uint32_t> last;
-        std::vector<uint32_t> order;
-        for (uint32_t i = 0; i < n; ++i) {
-            auto it = last.find(normal[i]);
-            if (it == last.end()) { last.emplace(normal[i], i); order.push_back(normal[i]); }
-            else it->second = i;
-        }
-        std::sort(order.begin(), order.end());
-        std::vector<uint32_t> at(order.size()), as(order.size());
-        for (size_t i = 0; i < order.size(); ++i) { at[i] = order[i]; as[i] = inv[last[order[i]]]; }
         e->upload(e->mur_coeff, sc);
         e->upload(e->mur_shifted, ss);
         e->upload(e->mur_apply_target, at); e->upload(e->mur_apply_src, as);
         e->mur_perm = perm;
         e->h_mur_apply = at;
         e->alloc(e->mur_saved, (size_t)n * 4);
-        e->mur_n = n; e->mur_napply = (uint32_t)order.size();
+        e->mur_n = n; e->mur_napply = (uint32_t)at.size();
         e->mur_on = n > 0;
         e->dirty();
     });
