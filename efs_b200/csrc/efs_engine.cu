@@ -705,7 +705,6 @@ struct efs_engine {
         sync("state sync");
     }
 
-    // group entries by target preserving order: returns unique targets + CSR offsets + permutation
     // Entries grouped by target: utarget ascending, group g = entries
     // perm[off[g] .. off[g+1]) in the caller's order (a stable sort by target).
     static void group_by(const std::vector<uint32_t>& tgt, std::vector<uint32_t>& utarget, std::vector<uint32_t>& off,
