@@ -1,0 +1,140 @@
+"""The served form's scheduling on the CPU (efs_b200/serve.py): the Server
+loop with stand-ins for the CUDA engine and batch, the request stream and
+the latency statistics.  The GPU behaviour (each result equal to the same
+request alone) is tests/test_gpu_serve.py; here the contract of the loop:
+every request runs exactly its step count, member slots and the HBM budget
+are respected (a request larger than the budget still runs, alone), arrival
+order is kept, and a chunk never runs past the nearest member's end."""
+import numpy as np
+import pytest
+
+from efs_b200 import serve
+
+
+class FakeEngine:
+    def __init__(self, device=0):
+        self.steps, self.bytes, self.destroyed = 0, 0, False
+
+    def initGPU(self):
+        return True
+
+    def deviceBytes(self):
+        return self.bytes
+
+    def computeEnergy(self, lagged=True):
+        return float(self.steps)
+
+    def destroy(self):
+        self.destroyed = True
+
+
+class FakeBatch:
+    log = []                                    # (members, steps, member bytes) per iterate
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        assert len(set(map(id, self.engines))) == len(self.engines)
+
+    def iterate(self, n):
+        FakeBatch.log.append((len(self.engines), n, sum(e.bytes for e in self.engines)))
+        for e in self.engines:
+            assert not e.destroyed
+            e.steps += n
+
+    def sync(self):
+        pass
+
+    def destroy(self):
+        pass
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    FakeBatch.log = []
+    monkeypatch.setattr(serve, "CudaEngine", FakeEngine)
+    monkeypatch.setattr(serve, "CudaBatch", FakeBatch)
+
+    def configure(engine, job):
+        engine.bytes = job["bytes"]
+        return None
+    monkeypatch.setattr(serve.workloads, "configure", configure)
+    return FakeBatch
+
+
+def job(side, nbytes):
+    return {"grid": [side, side, side], "bytes": nbytes}
+
+
+def drain(server, limit=10000):
+    for _ in range(limit):
+        if not server.round() and not server.waiting and not server.active:
+            return
+    raise AssertionError("server did not drain")
+
+
+def test_every_request_runs_its_steps_within_slots(fake):
+    s = serve.Server(hbm_budget=1e15, max_members=3, chunk=100)
+    steps = [250, 100, 730, 40, 333, 512, 99]
+    ids = [s.submit(job(16 + 8 * i, 1000), n, arrival=float(i)) for i, n in enumerate(steps)]
+    drain(s)
+    assert len(s.finished) == len(steps)
+    by_id = {r.rid: r for r in s.finished}
+    for rid, n in zip(ids, steps):
+        assert by_id[rid].result["energy"] == float(n)           # FakeEngine counts its timesteps
+        assert by_id[rid].engine is None
+    assert max(m for m, _, _ in fake.log) <= 3
+    assert max(n for _, n, _ in fake.log) <= 100
+    assert [r.rid for r in sorted(s.finished, key=lambda r: r.admitted)] == ids   # FIFO admission
+    assert s.used == 0
+
+
+def test_chunk_stops_at_the_nearest_end(fake):
+    s = serve.Server(hbm_budget=1e15, max_members=4, chunk=256)
+    s.submit(job(16, 10), 300, arrival=0.0)
+    s.submit(job(16, 10), 70, arrival=0.0)
+    s.round()                                    # admits both (nothing was running)
+    s.round()
+    assert fake.log[0][1] == 70                  # stops where the shorter one ends
+    drain(s)
+    assert sorted(r.result["energy"] for r in s.finished) == [70.0, 300.0]
+
+
+def test_hbm_budget(fake):
+    est = serve.estimate_bytes(job(64, 0))       # admission is decided on this estimate
+    budget = 2.5 * est                           # two 64^3 solves fit, a third does not
+    s = serve.Server(hbm_budget=budget, max_members=64, chunk=50)
+    for i in range(5):
+        s.submit(job(64, est), 120, arrival=float(i))
+    big = job(128, 0)
+    big["bytes"] = serve.estimate_bytes(big)     # larger than the whole budget
+    assert big["bytes"] > budget
+    huge = s.submit(big, 60, arrival=10.0)
+    drain(s)
+    assert len(s.finished) == 6
+    assert max(m for m, _, _ in fake.log) == 2
+    assert all(used <= budget for m, _, used in fake.log if m > 1)
+    lone = [m for m, _, used in fake.log if used > budget]
+    assert lone and all(m == 1 for m in lone)    # the oversize request ran, alone
+    assert any(r.rid == huge for r in s.finished)
+    assert s.used == 0
+
+
+def test_request_stream_and_latency_stats():
+    a = serve.request_stream(5.0, 20.0, seed=4)
+    b = serve.request_stream(5.0, 20.0, seed=4)
+    assert a == b and 60 <= len(a) <= 140
+    t = [x[0] for x in a]
+    assert all(0 < u < v for u, v in zip(t, t[1:])) and t[-1] < 20.0
+    assert all(s % 8 == 0 and 40 <= s <= 300 for _, _, s, _ in a)
+    assert all(5000 <= n <= 25000 for _, _, _, n in a)
+    frac = sum(k == "tfsf" for _, k, _, _ in a) / len(a)
+    assert 0.1 < frac < 0.5
+
+    class R:
+        def __init__(self, arrival, done):
+            self.arrival, self.done = arrival, done
+    st = serve.latency_stats([R(0.0, float(k)) for k in range(1, 101)])
+    assert st["completed"] == 100
+    assert st["p50_s"] == pytest.approx(np.percentile(np.arange(1, 101), 50))
+    assert st["p99_s"] == pytest.approx(np.percentile(np.arange(1, 101), 99))
+    assert serve.latency_stats([]) == {"completed": 0}
