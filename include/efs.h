@@ -232,7 +232,8 @@ efs_status efs_flush_energy(efs_engine* e, double* out);
  * (128 KB), held by every GPU that loads the library until the process
  * exits; a grid with more than 2^30 interior cells returns EFS_ERR_RANGE.
  * The first call on each device looks up the array's device address; make
- * that first call before any stream capture.  All calls on a device share
+ * that first call before any stream capture.  Devices with ordinals 0..63
+ * are served (EFS_ERR_RANGE above).  All calls on a device share
  * the array (each call writes what it reads, so nothing needs clearing):
  * calls that overlap on the GPU, e.g. two engines on one device driven from
  * two threads, race.  Sums in a different order than efs_energy (agrees to

@@ -1,8 +1,8 @@
 """Extract the golden vectors used by the parity tests from the reference's
 native-openEMS fixtures (reference tree: tests/fixtures/).
 
-Run in a checkout that has the reference at REF (default /root/reference);
-the outputs are committed so the tests never read the reference tree.
+Usage: python tests/golden/make_golden.py <reference checkout>
+The outputs are committed so the tests never read the reference tree.
   openems_cavity_vp.npy   engine_comparison/reference.json, engine "basic":
                           probe voltage vp, 251 samples every 2 steps from t=0
   openems_cavity_t.npy    the matching sample times (s)
@@ -17,7 +17,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <path of the reference checkout>")
+REF = sys.argv[1]
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 fx = os.path.join(REF, "tests", "fixtures")

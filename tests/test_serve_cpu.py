@@ -12,8 +12,10 @@ from efs_b200 import serve
 
 
 class FakeEngine:
+    energy_log = []                             # (grid side, reduction used) per retirement
     def __init__(self, device=0):
         self.steps, self.bytes, self.destroyed = 0, 0, False
+        self.numLines = [4, 4, 4]
 
     def initGPU(self):
         return True
@@ -22,6 +24,11 @@ class FakeEngine:
         return self.bytes
 
     def computeEnergy(self, lagged=True):
+        FakeEngine.energy_log.append((self.numLines[0], "alloc"))
+        return float(self.steps)
+
+    def energyNoAlloc(self):
+        FakeEngine.energy_log.append((self.numLines[0], "noalloc"))
         return float(self.steps)
 
     def destroy(self):
@@ -56,6 +63,7 @@ def fake(monkeypatch):
 
     def configure(engine, job):
         engine.bytes = job["bytes"]
+        engine.numLines = list(job.get("grid", (4, 4, 4)))
         return None
     monkeypatch.setattr(serve.workloads, "configure", configure)
     return FakeBatch
@@ -117,6 +125,19 @@ def test_hbm_budget(fake):
     assert lone and all(m == 1 for m in lone)    # the oversize request ran, alone
     assert any(r.rid == huge for r in s.finished)
     assert s.used == 0
+
+
+def test_retirement_energy_does_not_allocate(fake):
+    """Retiring a solve reads its energy through the allocation-free entry
+    point, so the retirement stays inside the budget the loop accounts for;
+    a grid beyond that entry point's fixed scratch (more than 2^30 interior
+    cells) uses the allocating reduction."""
+    FakeEngine.energy_log = []
+    s = serve.Server(hbm_budget=1e15, max_members=4, chunk=64)
+    s.submit(job(40, 1000), 10, arrival=0.0)
+    s.submit(job(1100, 1000), 10, arrival=0.0)   # 1099^3 > 2^30 interior cells
+    drain(s)
+    assert sorted(FakeEngine.energy_log) == [(40, "noalloc"), (1100, "alloc")]
 
 
 def test_request_stream_and_latency_stats():

@@ -3,11 +3,14 @@
 Some callers cannot let the library allocate device memory once they are
 running (a server that reserved its HBM budget up front, a host runtime that
 owns every device allocation).  efs_energy_noalloc serves them with scratch
-in a fixed array inside libefs.so.  These tests call it through the C ABI and
-check it against efs_energy (lagged == 0) at the energy tolerance the other
-tests use (1e-7 relative), twice in a row and again after the fields change,
-since every call shares the same scratch array.  The file runs last so that a
-failure here leaves every other test already run.
+in a fixed array inside libefs.so.  These tests call it through the C ABI:
+first on a fresh engine, before anything else could have allocated scratch
+for it, checking that neither the engine's device bytes nor the device's free
+memory change across the call; then against efs_energy (lagged == 0) to
+1e-10 relative (both sum the same f32 per-cell terms in f64, in different
+orders), twice in a row and again after the fields change, since every call
+shares the same scratch array.  The file runs last so that a failure here
+leaves every other test already run.
 """
 import ctypes as C
 
@@ -16,7 +19,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-7
+TOL = 1e-10
 
 
 def energy_ref(g):
@@ -44,15 +47,37 @@ def make_engine(cls, N, seed):
     return g
 
 
+def test_energy_noalloc_allocates_nothing(cuda_engine_cls):
+    import torch
+    warm = make_engine(cuda_engine_cls, (6, 6, 6), 3)
+    try:
+        energy_noalloc(warm)      # library code and the scratch address resident on this device
+    finally:
+        warm.destroy()
+    g = make_engine(cuda_engine_cls, (40, 36, 44), 5)
+    try:
+        torch.cuda.synchronize()
+        held, free = g.deviceBytes(), torch.cuda.mem_get_info()[0]
+        got = energy_noalloc(g)   # first energy call of this engine: no efs_energy before it
+        torch.cuda.synchronize()
+        assert g.deviceBytes() == held
+        assert torch.cuda.mem_get_info()[0] == free
+        ref = energy_ref(g)
+        assert abs(got - ref) <= TOL * abs(ref), (got, ref)
+    finally:
+        g.destroy()
+
+
 # (3,3,3): one partial sum; (48,50,64): 145,089 interior cells, three partial
-# sums, the last one partly filled; (8,1,1): no interior cells
-@pytest.mark.parametrize("N", [(3, 3, 3), (48, 50, 64), (8, 1, 1)])
+# sums, the last one partly filled; (4,2,43692): 131,073 = 2*65536+1 interior
+# cells, the last partial sum a single cell; (8,1,1): no interior cells
+@pytest.mark.parametrize("N", [(3, 3, 3), (48, 50, 64), (4, 2, 43692), (8, 1, 1)])
 def test_energy_noalloc_matches_energy(cuda_engine_cls, N):
     g = make_engine(cuda_engine_cls, N, 7)
     try:
         for _ in range(2):                        # two states of the fields
+            first, second = energy_noalloc(g), energy_noalloc(g)   # two calls in a row, before efs_energy
             ref = energy_ref(g)
-            first, second = energy_noalloc(g), energy_noalloc(g)   # two calls in a row
             for got in (first, second):
                 assert abs(got - ref) <= TOL * abs(ref), (N, got, ref)
             if ref == 0.0:
