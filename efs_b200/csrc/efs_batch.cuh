@@ -206,8 +206,6 @@ struct efs_batch {
         for (efs_engine* e : mem) {
             e->need_init();
             if (e->device != device) fail(EFS_ERR_INVALID, "batch members must share one device");
-            if (!e->tma_path())
-                fail(EFS_ERR_STATE, "batch members need the TMA-fed fused path (Nz % 4 == 0, EFS_CORE / EFS_FUSED unset)");
             if (e->ss_on || e->rlc_on || e->pbc_on)
                 fail(EFS_ERR_STATE, "batched stepping supports excitation, Mur, TFSF, ADE, UPML, NF2FF and the probe ring "
                                     "(not steady state, RLC or PBC)");

@@ -5,19 +5,27 @@
 // 1172, with the PBC and NF2FF/gather passes where WebGPUEngine.iterate puts
 // them, src/webgpu-engine.mjs:2448-2499) mapped onto kernels:
 //
-//   steady-state accumulate | ADE(volt) | Mur pre | RLC pre      (sparse)
-//   E update with UPML pre/post fused per cell                   (k_volt)
-//   TFSF(volt) | PBC(volt) | Mur post | excitation | Mur apply | RLC apply
-//   ADE(curr)                                                    (sparse)
-//   H update with UPML pre/post fused per cell                   (k_curr)
-//   TFSF(curr) | PBC(curr) | NF2FF accumulate | probe ring       (sparse)
+//   steady-state accumulate | ADE(volt) | Mur pre | RLC pre | ADE(curr)  (sparse)
+//   E of UPML cells (k_pml_e)
+//   E and H of every other cell in one pass (k_fused_tma)
+//   H of UPML cells (k_pml_h)
+//   TFSF(volt) | PBC(volt) | Mur post | excitation | Mur apply | RLC apply (sparse)
+//   [ADE apply to E]
+//   H of cells next to those E writes (k_deferred_h)
+//   TFSF(curr) | PBC(curr) | [ADE apply to H]                             (sparse)
+//   NF2FF sample/flush | probe ring
 //
 // Reads that the reference makes between the UPML pre-update and the core
 // update (ADE, Mur pre) are redirected to the region's flux array, which is
-// what the field holds at that moment, so fusing pre/post into the core
-// kernels keeps the reference's results.  Time-dependent parameters come
-// from a device-resident step counter, so `iterate(n)` replays a captured
-// CUDA graph of the whole step sequence.
+// what the field holds at that moment, so fusing pre/post into the UPML
+// passes keeps the reference's results.  Time-dependent parameters come from
+// a device-resident step counter, so `iterate(n)` replays a captured CUDA
+// graph of the whole step sequence.
+//
+// Device layout: NIJK with z rows padded to a multiple of 4 floats (pitch
+// Pz; efs_fused.cuh).  Every index a caller passes is in the reference's
+// unpadded NIJK order and is translated once, at configure time; field
+// transfers (getFields, uploadFields) repack rows with 2D copies.
 #include "../../include/efs.h"
 #include "efs_kernels.cuh"
 #include "efs_fused.cuh"
@@ -86,17 +94,16 @@ struct efs_engine {
 
     bool inited = false;
     uint32_t Nx = 0, Ny = 0, Nz = 0;
-    size_t N = 0;
+    size_t N = 0;               // cells of the caller's grid (component stride of caller indices)
+    uint32_t Pz = 0;            // device z pitch: Nz rounded up to a multiple of 4
+    size_t Nd = 0;              // device component stride Nx*Ny*Pz
     DevBuf volt, curr;          // fields (parity 0)
-    DevBuf volt_b, curr_b;      // second buffers of the fused path (parity 1)
-    bool fused = true;          // single-pass E+H kernel (else separate E and H sweeps)
+    DevBuf volt_b, curr_b;      // second buffers (parity 1): a step reads one parity and writes the other
     int cur = 0;                // parity holding the current fields
-    uint32_t xchunk = 32;       // x-planes per block of the fused kernel (EFS_XCHUNK)
-    int cpt = 1;                // z cells per thread of the fused kernel (1 or 2)
-    int ty_rows = 8;            // y rows per tile of the shared-memory fused kernel (8 or 16)
-    int fused_kind = 2;         // 2: TMA-fed fused kernel (needs Nz % 4 == 0, else 0), 0: register-blocked, 1: shared-memory tiled
-    int ry = 4;                 // y rows per thread of the register-blocked kernel (2, 4, 8)
-    DevBuf defer_bits, defer_rows, defer_cells;
+    uint32_t xchunk = 32;       // x-planes per CTA of the fused kernel (EFS_XCHUNK)
+    uint64_t wait_ns = 1000000000ull;   // limit of the fused kernel's bounded waits
+    uint32_t skip_plane = ~0u;          // diagnostics (efs_debug_set_wait): a plane whose loads are never issued
+    DevBuf defer_cells;
     uint32_t defer_n = 0;
     std::vector<uint32_t> h_exc_targets, h_tfsf_v_targets, h_mur_apply, h_rlc_series;
     bool indexed = false;
@@ -123,11 +130,36 @@ struct efs_engine {
     std::vector<std::unique_ptr<Region>> pml;
     DevBuf vflux_ptrs[2], cflux_ptrs[2];
 
-    float* vbuf(int p) const { return (p && volt_b.p) ? volt_b.as<float>() : volt.as<float>(); }
-    float* cbuf(int p) const { return (p && curr_b.p) ? curr_b.as<float>() : curr.as<float>(); }
+    float* vbuf(int p) const { return p ? volt_b.as<float>() : volt.as<float>(); }
+    float* cbuf(int p) const { return p ? curr_b.as<float>() : curr.as<float>(); }
     float* vcur() const { return vbuf(cur); }
     float* ccur() const { return cbuf(cur); }
-    int pnext(int p) const { return fused ? 1 - p : p; }
+    static int pnext(int p) { return 1 - p; }
+
+    // Caller index (n*N + x*Ny*Nz + y*Nz + z, the reference's NIJK order) ->
+    // device index (n*Nd + (x*Ny + y)*Pz + z).
+    uint32_t dev_index(uint32_t f) const {
+        const uint64_t n = f / N, cell = f - n * N, nyz = (uint64_t)Ny * Nz;
+        const uint64_t x = cell / nyz, r = cell - x * nyz, y = r / Nz, z = r - y * Nz;
+        return (uint32_t)(n * Nd + (x * Ny + y) * Pz + z);
+    }
+    size_t dev_cell(uint64_t x, uint64_t y, uint64_t z) const { return (size_t)((x * Ny + y) * Pz + z); }
+    // Host array of `comps` components in the caller's layout -> device
+    // buffer in the padded layout (pad cells zero).
+    void upload_padded(DevBuf& b, const void* src, size_t comps, size_t elem = 4) {
+        alloc(b, comps * Nd * elem, Pz != Nz);
+        ck(cudaMemcpy2DAsync(b.p, (size_t)Pz * elem, src, (size_t)Nz * elem, (size_t)Nz * elem, comps * Nx * Ny,
+                             cudaMemcpyHostToDevice, stream), "upload (padded rows)");
+        sync("upload sync");
+    }
+    void copy_fields_out(float* dst, const float* dev) {
+        ck(cudaMemcpy2DAsync(dst, (size_t)Nz * 4, dev, (size_t)Pz * 4, (size_t)Nz * 4, 3 * (size_t)Nx * Ny,
+                             cudaMemcpyDeviceToHost, stream), "read fields");
+    }
+    void copy_fields_in(float* dev, const float* src) {
+        ck(cudaMemcpy2DAsync(dev, (size_t)Pz * 4, src, (size_t)Nz * 4, (size_t)Nz * 4, 3 * (size_t)Nx * Ny,
+                             cudaMemcpyHostToDevice, stream), "write fields");
+    }
 
     // Mur (host copies kept to rebuild read redirects)
     bool mur_on = false;
@@ -269,25 +301,16 @@ struct efs_engine {
             if (p[i] >= 3 * N) fail(EFS_ERR_INVALID, std::string(what) + ": index out of range");
     }
 
-    Grid grid(int p = 0) const {
-        Grid g;
-        g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.indexed = indexed;
-        g.N = N; g.NyNz = (size_t)Ny * Nz;
-        g.volt = vbuf(p); g.curr = cbuf(p);
-        g.mat = mat.as<uint32_t>(); g.table = table.as<float>();
-        g.vv = vv.as<float>(); g.vi = vi.as<float>(); g.ii = ii.as<float>(); g.iv = iv.as<float>();
-        return g;
-    }
     FusedGrid fused_grid(int p) const {
         FusedGrid g;
-        g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.xchunk = xchunk;
-        g.N = N; g.NyNz = (size_t)Ny * Nz;
+        g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.xchunk = xchunk; g.Pz = Pz;
+        g.N = Nd; g.NyNz = (size_t)Ny * Pz;
         g.V0 = vbuf(p); g.H0 = cbuf(p); g.V1 = vbuf(1 - p); g.H1 = cbuf(1 - p);
         g.mat = mat.as<uint32_t>(); g.table = table.as<float>();
         g.vv = vv.as<float>(); g.vi = vi.as<float>(); g.ii = ii.as<float>(); g.iv = iv.as<float>();
-        g.defer = defer_n ? defer_bits.as<uint32_t>() : nullptr;
-        g.defer_rows = defer_n ? defer_rows.as<uint32_t>() : nullptr;
         g.status = d_status;
+        g.wait_ns = wait_ns;
+        g.skip_plane = skip_plane;
         return g;
     }
     // UPML set whose flux pointers are the parity-p buffers
@@ -307,14 +330,15 @@ struct efs_engine {
         return s;
     }
 
-    // Location a read sees after the UPML pre-update: the flux slot of the
-    // last region containing the cell, else the field itself.
+    // Location a read of device field index `field_idx` sees after the UPML
+    // pre-update: the flux slot of the last region containing the cell, else
+    // the field itself.
     ReadLoc redirect(uint32_t field_idx) const {
-        uint32_t n = field_idx / (uint32_t)N;
-        size_t cell = field_idx - (size_t)n * N;
-        uint32_t x = (uint32_t)(cell / ((size_t)Ny * Nz));
-        uint32_t y = (uint32_t)((cell / Nz) % Ny);
-        uint32_t z = (uint32_t)(cell % Nz);
+        uint32_t n = field_idx / (uint32_t)Nd;
+        size_t cell = field_idx - (size_t)n * Nd;
+        uint32_t x = (uint32_t)(cell / ((size_t)Ny * Pz));
+        uint32_t y = (uint32_t)((cell / Pz) % Ny);
+        uint32_t z = (uint32_t)(cell % Pz);
         ReadLoc l{0, field_idx};
         for (size_t r = 0; r < pml.size(); ++r) {
             const Region& R = *pml[r];
@@ -374,20 +398,18 @@ struct efs_engine {
         plan_dirty = false;
     }
 
-    // Fused path: H cells whose curl reads an E value rewritten by a sparse
-    // post-update operation (TFSF, PBC, Mur apply, excitation, series RLC)
-    // are updated after those operations by k_deferred_h.
+    // H cells whose curl reads an E value rewritten by a sparse post-update
+    // operation (TFSF, PBC, Mur apply, excitation, series RLC) are updated
+    // after those operations by k_deferred_h.  Targets are device indices.
     void build_deferred() {
         defer_n = 0;
-        if (!fused) return;
-        std::vector<uint32_t> mod;   // modified E entries as n*N + cell
+        std::vector<uint32_t> mod;   // modified E entries as n*Nd + device cell
         auto add = [&](const std::vector<uint32_t>& v) { mod.insert(mod.end(), v.begin(), v.end()); };
         if (tfsf_on) add(h_tfsf_v_targets);
         if (exc_on) add(h_exc_targets);
         if (mur_on) add(h_mur_apply);
         if (rlc_on) add(h_rlc_series);
         const uint32_t nl[3] = {Nx, Ny, Nz};
-        const size_t NyNz = (size_t)Ny * Nz;
         if (pbc_on)
             for (auto& a : pbc_axes) {
                 uint32_t t0 = (a.axis + 1) % 3, t1 = (a.axis + 2) % 3;
@@ -396,22 +418,23 @@ struct efs_engine {
                         uint32_t p[3];
                         p[a.axis] = 0; p[t0] = i0; p[t1] = i1;
                         if (a.axis == 1) { p[0] = i1; p[2] = i0; }   // face_to_grid order of the reference
-                        size_t c = p[0] * NyNz + (size_t)p[1] * Nz + p[2];
-                        mod.push_back((uint32_t)(t0 * N + c));
-                        mod.push_back((uint32_t)(t1 * N + c));
+                        const size_t c = dev_cell(p[0], p[1], p[2]);
+                        mod.push_back((uint32_t)(t0 * Nd + c));
+                        mod.push_back((uint32_t)(t1 * Nd + c));
                     }
             }
         if (mod.empty()) return;
-        std::vector<uint32_t> bits((N + 31) / 32, 0);
+        const size_t NyPz = (size_t)Ny * Pz;
+        std::vector<uint32_t> bits((Nd + 31) / 32, 0);
         auto mark = [&](int64_t x, int64_t y, int64_t z) {
             if (x < 0 || y < 0 || z < 0) return;
-            size_t c = (size_t)x * NyNz + (size_t)y * Nz + (size_t)z;
+            const size_t c = dev_cell(x, y, z);
             bits[c >> 5] |= 1u << (c & 31);
         };
         for (uint32_t f : mod) {
-            uint32_t n = f / (uint32_t)N;
-            size_t cell = f - (size_t)n * N;
-            int64_t x = cell / NyNz, y = (cell / Nz) % Ny, z = cell % Nz;
+            const uint32_t n = f / (uint32_t)Nd;
+            const size_t cell = f - (size_t)n * Nd;
+            const int64_t x = cell / NyPz, y = (cell / Pz) % Ny, z = cell % Pz;
             // E_n(m) appears in the curls of H at m, m - e_a, m - e_b (a, b != n)
             mark(x, y, z);
             if (n != 0) mark(x - 1, y, z);
@@ -421,26 +444,15 @@ struct efs_engine {
         std::vector<uint32_t> cells;
         for (size_t w = 0; w < bits.size(); ++w)
             for (uint32_t b = bits[w]; b; b &= b - 1) cells.push_back((uint32_t)(w * 32 + __builtin_ctz(b)));
-        // row summary: bit y of plane x set when row (x, y) holds a deferred cell
-        const uint32_t rw = (Ny + 31) / 32;
-        std::vector<uint32_t> rows((size_t)Nx * rw, 0);
-        for (uint32_t c : cells) {
-            const size_t xy = c / Nz;
-            const uint32_t x = (uint32_t)(xy / Ny), y = (uint32_t)(xy % Ny);
-            rows[(size_t)x * rw + (y >> 5)] |= 1u << (y & 31);
-        }
-        upload(defer_rows, rows);
-        upload(defer_bits, bits);
         upload(defer_cells, cells);
         defer_n = (uint32_t)cells.size();
     }
 
     // Enqueue timestep k of a batch (numTS = state.numTS + k); the fields are
-    // read from parity p and, on the fused path, written to parity 1 - p.
+    // read from parity p and written to parity 1 - p.
     // `last`: k is the batch's final step (buffered NF2FF samples are flushed).
     void enqueue_step(uint32_t k, int p, bool last) {
         const int q = pnext(p);
-        const Grid g = grid(p);
         const PmlSet ps = pml_set(p);
         const PmlSet pn = pml_set(q);
         StepState* st = state.as<StepState>();
@@ -462,18 +474,12 @@ struct efs_engine {
         RlcDev rd = rlc_dev();
         if (rlc_on) k_rlc_pre<<<blocks(rlc_n, T), T, 0, stream>>>(rd);
         const bool hp = !pml.empty();
-        if (fused) {
-            // ADE(curr) reads H and the current flux, which the E side never
-            // touches: it runs before the fused kernel overwrites the flux.
-            if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
-            if (pml_split()) launch_pml_e(p);
-            launch_fused(p);
-            if (pml_split()) launch_pml_h(p);
-        } else {
-            dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
-            if (indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, stream>>>(g, ps); }
-            else { if (hp) k_volt<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, stream>>>(g, ps); }
-        }
+        // ADE(curr) reads H and the current flux, which the E side never
+        // touches: it runs before the fused kernel overwrites the flux.
+        if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+        if (hp) launch_pml_e(p);
+        launch_fused_tma(p);
+        if (hp) launch_pml_h(p);
         // --- post-voltage / apply (on the updated E) ---
         if (tfsf_on && tfsf_v.groups) k_point_sources<1><<<blocks(tfsf_v.groups, T), T, 0, stream>>>(V1, st, k, point_dev(tfsf_v, tfsf_signal, tfsf_len, tfsf_period));
         if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, true, V1);
@@ -485,20 +491,11 @@ struct efs_engine {
         }
         if (mur_on) k_mur_apply<<<blocks(mur_napply, T), T, 0, stream>>>(V1, md);
         if (rlc_on) k_rlc_apply<<<blocks(rlc_groups, T), T, 0, stream>>>(V1, rd);
-        if (fused) {
-            if (defer_n) {
-                const FusedGrid fg = fused_grid(p);
-                const uint32_t* cells = defer_cells.as<uint32_t>();
-                if (indexed) { if (hp) k_deferred_h<true, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<true, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
-                else { if (hp) k_deferred_h<false, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<false, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
-            }
-        } else {
-            // --- pre-current ---
-            if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
-            // --- core H (+UPML) ---
-            dim3 cb(CORE_BZ, CORE_BY), cg(blocks(Nz, CORE_BZ), blocks(Ny, CORE_BY), blocks(Nx, CORE_TX));
-            if (indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, stream>>>(g, ps); }
-            else { if (hp) k_curr<false, true><<<cg, cb, 0, stream>>>(g, ps); else k_curr<false, false><<<cg, cb, 0, stream>>>(g, ps); }
+        if (defer_n) {
+            const FusedGrid fg = fused_grid(p);
+            const uint32_t* cells = defer_cells.as<uint32_t>();
+            if (indexed) { if (hp) k_deferred_h<true, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<true, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
+            else { if (hp) k_deferred_h<false, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<false, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
         }
         // --- post-current (on the updated H) ---
         if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C1, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
@@ -515,40 +512,9 @@ struct efs_engine {
     }
     RingDev ring_dev() const { return RingDev{ring_idx.as<uint32_t>(), ring_n, ring_interval, ring_q0, ring_max, ring.as<float>()}; }
 
-    template <bool IDX, bool PML, int CPT, int TY>
-    void launch_fused_k(dim3 g, dim3 b, const FusedGrid& fg, const PmlSet& ps, const PmlSet& pn) {
-        const size_t sm = sizeof(FusedSmem<CPT, TY>);
-        static bool attr_set = false;   // per instantiation; the attribute is per kernel, all devices alike
-        if (!attr_set) {
-            ck(cudaFuncSetAttribute(k_fused<IDX, PML, CPT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attr");
-            attr_set = true;
-        }
-        k_fused<IDX, PML, CPT, TY><<<g, b, sm, stream>>>(fg, ps, pn);
-    }
-    template <int CPT, int TY>
-    void launch_fused_t(int p) {
-        const FusedGrid fg = fused_grid(p);
-        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
-        dim3 b(32, TY + 1), g(blocks(Nz, 32 * CPT), blocks(Ny, TY), blocks(Nx, xchunk));
-        const bool hp = !pml.empty();
-        if (indexed) { if (hp) launch_fused_k<true, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<true, false, CPT, TY>(g, b, fg, ps, pn); }
-        else { if (hp) launch_fused_k<false, true, CPT, TY>(g, b, fg, ps, pn); else launch_fused_k<false, false, CPT, TY>(g, b, fg, ps, pn); }
-    }
-    template <int RY, typename IT>
-    void launch_fused_reg_k(dim3 g, dim3 b, const FusedGrid& fg, const PmlSet& ps, const PmlSet& pn) {
-        const bool hp = !pml.empty();
-        if (indexed) { if (hp) k_fused_reg<true, true, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<true, false, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); }
-        else { if (hp) k_fused_reg<false, true, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); else k_fused_reg<false, false, RY, IT><<<g, b, 0, stream>>>(fg, ps, pn); }
-    }
-    template <int RY>
-    void launch_fused_reg(int p) {
-        const FusedGrid fg = fused_grid(p);
-        const PmlSet ps = pml_set(p), pn = pml_set(1 - p);
-        dim3 b(32, 4), g(blocks(Nz, RZ), blocks(Ny, 4 * RY), blocks(Nx, xchunk));
-        launch_fused_reg_k<RY, uint32_t>(g, b, fg, ps, pn);   // efs_init guarantees 3*N < 2^32
-    }
     // TMA-fed kernel: tensor maps over this parity's fields and the material
-    // rows, boxes of one tile plus halos (efs_tma.cuh)
+    // rows (the grid's Nz x Ny x Nx cells over the padded layout), boxes of
+    // one tile plus halos (efs_tma.cuh)
     CUtensorMap tensor_map(const void* base, CUtensorMapDataType dt, uint32_t rank, const uint32_t box[4]) const {
         static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
         if (!encode) {
@@ -559,7 +525,7 @@ struct efs_engine {
             encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
         }
         const cuuint64_t dims[4] = {Nz, Ny, Nx, 3};
-        const cuuint64_t strides[3] = {(cuuint64_t)Nz * 4, (cuuint64_t)Ny * Nz * 4, (cuuint64_t)N * 4};
+        const cuuint64_t strides[3] = {(cuuint64_t)Pz * 4, (cuuint64_t)Ny * Pz * 4, (cuuint64_t)Nd * 4};
         const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
         const cuuint32_t es[4] = {1, 1, 1, 1};
         CUtensorMap m;
@@ -591,9 +557,8 @@ struct efs_engine {
         if (indexed) { if (hp) launch_fused_tma_k<true, true>(g, tH, tE, tM, fg, ps); else launch_fused_tma_k<true, false>(g, tH, tE, tM, fg, ps); }
         else { if (hp) launch_fused_tma_k<false, true>(g, tH, tE, tM, fg, ps); else launch_fused_tma_k<false, false>(g, tH, tE, tM, fg, ps); }
     }
-    // TMA path with UPML: region cells are updated by k_pml_e / k_pml_h around the fused kernel
-    bool tma_path() const { return fused && fused_kind == 2 && Nz % 4 == 0; }
-    bool pml_split() const { return tma_path() && !pml.empty(); }
+    // UPML cells are updated by k_pml_e / k_pml_h around the fused kernel
+    bool pml_split() const { return !pml.empty(); }
     uint32_t pml_items() const {   // work items of k_pml_e / k_pml_h: PML_ZC cells of a region row each
         size_t t = 0;
         for (auto& r : pml) t += (size_t)r->n[0] * r->n[1] * ((r->n[2] + PML_ZC - 1) / PML_ZC);
@@ -612,20 +577,6 @@ struct efs_engine {
         const uint32_t t = pml_items(), T = 256;
         if (indexed) k_pml_h<true><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, t);
         else k_pml_h<false><<<blocks(t, T), T, 0, stream>>>(fg, ps, pn, t);
-    }
-    void launch_fused(int p) {
-        if (tma_path()) {
-            launch_fused_tma(p);
-            return;
-        }
-        if (fused_kind != 1) {
-            if (ry >= 8) launch_fused_reg<8>(p);
-            else if (ry >= 4) launch_fused_reg<4>(p);
-            else launch_fused_reg<2>(p);
-            return;
-        }
-        if (cpt >= 2) { if (ty_rows >= 16) launch_fused_t<2, 16>(p); else launch_fused_t<2, 8>(p); }
-        else { if (ty_rows >= 16) launch_fused_t<1, 16>(p); else launch_fused_t<1, 8>(p); }
     }
 
     PointSources point_dev(const PointSet& p, const DevBuf& sig, uint32_t len, uint32_t period) const {
@@ -653,7 +604,7 @@ struct efs_engine {
         p.fs0 = nl[t0]; p.fs1 = nl[t1];
         p.b0 = isVolt ? p.fs0 : p.fs0 - 1; p.b1 = isVolt ? p.fs1 : p.fs1 - 1;
         p.src = isVolt ? nl[a.axis] - 2 : 0; p.dst = isVolt ? 0 : nl[a.axis] - 2;
-        p.Nx = Nx; p.Ny = Ny; p.Nz = Nz; p.cosP = a.c; p.sinP = a.s;
+        p.Nx = Nx; p.Ny = Ny; p.Nz = Nz; p.Pz = Pz; p.cosP = a.c; p.sinP = a.s;
         p.imag = pbc_imag.as<float>() + a.imag_off;
         dim3 b(16, 16), gr(blocks(p.b0, 16), blocks(p.b1, 16));
         if (p.b0 && p.b1) k_pbc<<<gr, b, 0, stream>>>(F, p);
@@ -668,7 +619,7 @@ struct efs_engine {
             cudaGraphExec_t ge = graph_for(m, cur);
             ck(cudaGraphLaunch(ge, stream), "cudaGraphLaunch");
             numTS += m;
-            if (fused && (m & 1)) cur ^= 1;
+            if (m & 1) cur ^= 1;
             n -= m;
         }
         ck(cudaGetLastError(), "iterate");
@@ -747,35 +698,27 @@ efs_status guard(efs_engine* e, F&& f) {
 void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     if (!dims || dims[0] == 0 || dims[1] == 0 || dims[2] == 0) fail(EFS_ERR_INVALID, "grid dimensions must be positive");
     size_t N = (size_t)dims[0] * dims[1] * dims[2];
-    if (3 * N >= (1ull << 32)) fail(EFS_ERR_RANGE, "grid too large for 32-bit field indices (3*Nx*Ny*Nz >= 2^32)");
+    const uint32_t Pz = (dims[2] + 3u) & ~3u;
+    const size_t Nd = (size_t)dims[0] * dims[1] * Pz;
+    if (3 * Nd >= (1ull << 32))
+        fail(EFS_ERR_RANGE, "grid too large for 32-bit field indices (3*Nx*Ny*Pz >= 2^32, Pz = Nz rounded up to a multiple of 4)");
     // a fresh init drops every extension
     e->drop_graphs();
     e->pml.clear();
     e->exc_on = e->mur_on = e->tfsf_on = e->ade_on = e->rlc_on = e->ss_on = e->pbc_on = e->ring_on = e->nf_on = false;
     e->ade_v = efs_engine::AdeSide(); e->ade_c = efs_engine::AdeSide();
     e->gd_n = 0;
-    e->Nx = dims[0]; e->Ny = dims[1]; e->Nz = dims[2]; e->N = N;
+    e->Nx = dims[0]; e->Ny = dims[1]; e->Nz = dims[2]; e->N = N; e->Pz = Pz; e->Nd = Nd;
     e->h_exc_targets.clear(); e->h_tfsf_v_targets.clear(); e->h_mur_apply.clear(); e->h_rlc_series.clear();
     e->defer_n = 0;
-    // core path and fused-kernel shape: EFS_CORE=split selects separate E/H sweeps
-    const char* core = getenv("EFS_CORE");
-    e->fused = !(core && std::string(core) == "split");
+    // plane depth (x-planes per CTA) of the fused kernel; results do not depend on it
+    e->xchunk = 32;
     if (const char* s = getenv("EFS_XCHUNK")) e->xchunk = std::max(1, atoi(s));
-    if (const char* s = getenv("EFS_CPT")) e->cpt = std::max(1, atoi(s));
-    if (const char* s = getenv("EFS_TY")) e->ty_rows = std::max(8, atoi(s));
-    e->fused_kind = 2;
-    if (const char* s = getenv("EFS_FUSED")) e->fused_kind = std::string(s) == "smem" ? 1 : std::string(s) == "reg" ? 0 : 2;
-    if (const char* s = getenv("EFS_RY")) e->ry = std::max(2, atoi(s));
     e->cur = 0;
-    e->alloc(e->volt, 3 * N * sizeof(float));
-    e->alloc(e->curr, 3 * N * sizeof(float));
-    if (e->fused) {
-        e->alloc(e->volt_b, 3 * N * sizeof(float));
-        e->alloc(e->curr_b, 3 * N * sizeof(float));
-    } else {
-        e->volt_b.reset();
-        e->curr_b.reset();
-    }
+    e->alloc(e->volt, 3 * Nd * sizeof(float));
+    e->alloc(e->curr, 3 * Nd * sizeof(float));
+    e->alloc(e->volt_b, 3 * Nd * sizeof(float));
+    e->alloc(e->curr_b, 3 * Nd * sizeof(float));
     e->alloc(e->state, sizeof(StepState));
     e->numTS = 0;
     e->hstate = StepState{};
@@ -841,7 +784,8 @@ efs_status efs_init(efs_engine* e, const uint32_t dims[3], const float* vv, cons
         if (!vv || !vi || !ii || !iv) fail(EFS_ERR_INVALID, "coefficient arrays must be non-null");
         alloc_fields(e, dims);
         const size_t N = e->N;
-        // Deduplicate per-cell (vv,vi,ii,iv) x 3 tuples into a material table.
+        // Deduplicate per-cell (vv,vi,ii,iv) x 3 tuples into a material table
+        // (material index per cell in the caller's layout; padded on upload).
         std::unordered_map<std::array<uint32_t, 12>, uint32_t, TupleHash> ids;
         std::vector<uint32_t> mat(N);
         std::vector<float> table;
@@ -867,12 +811,12 @@ efs_status efs_init(efs_engine* e, const uint32_t dims[3], const float* vv, cons
         if (ok) {
             e->indexed = true;
             e->ntable = (uint32_t)ids.size();
-            e->upload(e->mat, mat);
+            e->upload_padded(e->mat, mat.data(), 1);
             e->upload(e->table, table);
         } else {
             e->indexed = false;
-            e->upload(e->vv, vv, 3 * N); e->upload(e->vi, vi, 3 * N);
-            e->upload(e->ii, ii, 3 * N); e->upload(e->iv, iv, 3 * N);
+            e->upload_padded(e->vv, vv, 3); e->upload_padded(e->vi, vi, 3);
+            e->upload_padded(e->ii, ii, 3); e->upload_padded(e->iv, iv, 3);
         }
         e->sync_state_to_device();
         e->inited = true;
@@ -888,7 +832,7 @@ efs_status efs_init_indexed(efs_engine* e, const uint32_t dims[3], const uint32_
             if (mat[c] >= ntable) fail(EFS_ERR_INVALID, "material index out of range");
         e->indexed = true;
         e->ntable = ntable;
-        e->upload(e->mat, mat, e->N);
+        e->upload_padded(e->mat, mat, 1);
         e->upload(e->table, table, (size_t)ntable * 12);
         e->sync_state_to_device();
         e->inited = true;
@@ -905,7 +849,7 @@ efs_status efs_configure_excitation(efs_engine* e, const float* signal, uint32_t
         std::vector<uint32_t> tgt(count);
         for (uint32_t i = 0; i < count; ++i) {
             if (dir[i] > 2 || pos[i] >= e->N) fail(EFS_ERR_INVALID, "excitation dir/pos out of range");
-            tgt[i] = dir[i] * (uint32_t)e->N + pos[i];
+            tgt[i] = e->dev_index(dir[i] * (uint32_t)e->N + pos[i]);
         }
         std::vector<uint32_t> ut, off, perm;
         efs_engine::group_by(tgt, ut, off, perm);
@@ -998,7 +942,7 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
             e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
             compact_pml(e, *R, in);
             e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
-            if (e->fused) { e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4); }
+            e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4);
             out.push_back(std::move(R));
         }
         // the per-cell UPML chain keeps at most PML_MAX_OVERLAP regions in registers:
@@ -1033,12 +977,12 @@ efs_status efs_configure_mur(efs_engine* e, const float* coeff, const uint32_t* 
         // face across rows).  The pre and post updates are per entry; apply
         // resolves each target to its last writer in the caller's order
         // (sequential loop :1016-1023), which the permutation leaves intact.
-        std::vector<uint32_t> perm(n), sn(normal, normal + n);
-        for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+        std::vector<uint32_t> perm(n), sn(n);
+        for (uint32_t i = 0; i < n; ++i) { perm[i] = i; sn[i] = e->dev_index(normal[i]); }
         efs_engine::radix_sort_pairs(sn, perm);           // stable: equal normals keep the caller's order
         std::vector<uint32_t> ss(n);
         std::vector<float> sc(n);
-        for (uint32_t k = 0; k < n; ++k) { ss[k] = shifted[perm[k]]; sc[k] = coeff[perm[k]]; }
+        for (uint32_t k = 0; k < n; ++k) { ss[k] = e->dev_index(shifted[perm[k]]); sc[k] = coeff[perm[k]]; }
         // apply: per distinct normal (ascending) its last writer in the caller's
         // order, which is the last entry of its run in the sorted order
         std::vector<uint32_t> at, as;
@@ -1062,6 +1006,7 @@ static void build_points(efs_engine* e, efs_engine::PointSet& ps, const efs_tfsf
     std::vector<uint32_t> tgt(n);
     for (uint32_t i = 0; i < n; ++i) tgt[i] = pts[i].field_idx;
     e->check_idx3(tgt.data(), n, "TFSF field_idx");
+    for (uint32_t i = 0; i < n; ++i) tgt[i] = e->dev_index(tgt[i]);
     std::vector<uint32_t> ut, off, perm;
     efs_engine::group_by(tgt, ut, off, perm);
     std::vector<uint32_t> d(n);
@@ -1079,7 +1024,7 @@ efs_status efs_configure_tfsf(efs_engine* e, const float* signal, uint32_t L, ui
         if ((nv && !vp) || (nc && !cp)) fail(EFS_ERR_INVALID, "TFSF point arrays must be non-null");
         build_points(e, e->tfsf_v, vp, nv);
         e->h_tfsf_v_targets.clear();
-        for (uint32_t i = 0; i < nv; ++i) e->h_tfsf_v_targets.push_back(vp[i].field_idx);
+        for (uint32_t i = 0; i < nv; ++i) e->h_tfsf_v_targets.push_back(e->dev_index(vp[i].field_idx));
         build_points(e, e->tfsf_c, cp, nc);
         e->upload(e->tfsf_signal, signal, L);
         e->tfsf_len = L; e->tfsf_period = period;
@@ -1112,7 +1057,7 @@ efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order*
                     const float* c = side == 0 ? dr.v_lor : dr.i_lor;
                     for (uint32_t i = 0; i < od.num_cells; ++i) {
                         if (dr.pos_idx[i] >= e->N) fail(EFS_ERR_INVALID, "ADE pos_idx out of range");
-                        s.h_field.push_back(dr.dir * (uint32_t)e->N + dr.pos_idx[i]);
+                        s.h_field.push_back(e->dev_index(dr.dir * (uint32_t)e->N + dr.pos_idx[i]));
                         const float k0 = a ? a[i] : 0.f, k1 = b ? b[i] : 0.f, k2 = c ? c[i] : 0.f;
                         const std::array<uint32_t, 4> key{bits(k0), bits(k1), bits(k2), od.has_lorentz ? 1u : 0u};
                         if (tuples.empty() || key != last) {
@@ -1149,7 +1094,7 @@ efs_status efs_configure_rlc(efs_engine* e, uint32_t n, const efs_rlc_element* e
         std::vector<float> p(9 * (size_t)n);
         for (uint32_t i = 0; i < n; ++i) {
             if (el[i].direction > 2 || el[i].field_idx >= e->N) fail(EFS_ERR_INVALID, "RLC field_idx/direction out of range");
-            tgt[i] = el[i].direction * (uint32_t)e->N + el[i].field_idx;
+            tgt[i] = e->dev_index(el[i].direction * (uint32_t)e->N + el[i].field_idx);
             type[i] = el[i].type_flag;
             const float v[9] = {el[i].i2v, el[i].ilv, el[i].vvd, el[i].vv2, el[i].vj1, el[i].vj2, el[i].ib0, el[i].b1, el[i].b2};
             memcpy(&p[9 * (size_t)i], v, sizeof(v));
@@ -1201,7 +1146,9 @@ efs_status efs_configure_steady_state(efs_engine* e, const uint32_t* idx, uint32
         e->need_init();
         if (n && !idx) fail(EFS_ERR_INVALID, "probe_idx must be non-null");
         e->check_idx3(idx, n, "steady-state probe_idx");
-        e->upload(e->ss_idx, idx, n);
+        std::vector<uint32_t> di(n);
+        for (uint32_t i = 0; i < n; ++i) di[i] = e->dev_index(idx[i]);
+        e->upload(e->ss_idx, di);
         e->alloc(e->ss_e1, (size_t)n * 4); e->alloc(e->ss_e2, (size_t)n * 4);
         e->ss_n = n; e->ss_period = period; e->ss_threshold = threshold > 0 ? threshold : 1e-6f;
         e->ss_on = n > 0; e->ss_recording = false; e->ss_count_before = 0;
@@ -1277,7 +1224,9 @@ efs_status efs_configure_probe_gather(efs_engine* e, const uint32_t* idx, uint32
         if (n == 0) return;   // the reference returns without configuring (:2578)
         if (!idx) fail(EFS_ERR_INVALID, "indices must be non-null");
         e->check_idx3(idx, n, "probe index");
-        e->upload(e->gd_idx, idx, n);
+        std::vector<uint32_t> di(n);
+        for (uint32_t i = 0; i < n; ++i) di[i] = e->dev_index(idx[i]);
+        e->upload(e->gd_idx, di);
         e->alloc(e->gd_out, 2 * (size_t)n * 4);
         e->gd_n = n;
     });
@@ -1303,7 +1252,9 @@ efs_status efs_configure_probe_gather_buffered(efs_engine* e, const uint32_t* id
         if (!idx) fail(EFS_ERR_INVALID, "indices must be non-null");
         if (interval == 0) fail(EFS_ERR_INVALID, "sample_interval must be > 0");
         e->check_idx3(idx, n, "probe index");
-        e->upload(e->ring_idx, idx, n);
+        std::vector<uint32_t> di(n);
+        for (uint32_t i = 0; i < n; ++i) di[i] = e->dev_index(idx[i]);
+        e->upload(e->ring_idx, di);
         e->alloc(e->ring, (size_t)maxS * n * 2 * 4);
         e->ring_n = n; e->ring_max = maxS; e->ring_interval = interval;
         e->ring_q0 = e->numTS / interval;    // multiples already passed at configure time
@@ -1346,7 +1297,7 @@ efs_status efs_configure_nf2ff(efs_engine* e, const uint32_t* pts, uint32_t np, 
         Nf2ffDev& d = e->nf;
         memset(&d, 0, sizeof(d));
         d.np = np; d.nf = nf; d.maxTS = maxTS; d.window = window;
-        d.Nx = e->Nx; d.Ny = e->Ny; d.Nz = e->Nz;
+        d.Nx = e->Nx; d.Ny = e->Ny; d.Nz = e->Nz; d.Pz = e->Pz;
         const uint32_t nl[3] = {e->Nx, e->Ny, e->Nz};
         uint32_t o = 0;
         for (int k = 0; k < 6; ++k) { d.off[k] = o; o += nl[k % 3]; }
@@ -1429,7 +1380,7 @@ static void energy_launch(efs_engine* e, int slot) {
     if (e->Nx < 2 || e->Ny < 2 || e->Nz < 2) {
         ck(cudaMemsetAsync(res, 0, sizeof(double), e->stream), "memset");
     } else {
-        k_energy<<<1024, 256, 0, e->stream>>>(e->vcur(), e->ccur(), e->Nx, e->Ny, e->Nz, e->en_partial.as<double>());
+        k_energy<<<1024, 256, 0, e->stream>>>(e->vcur(), e->ccur(), e->Nx, e->Ny, e->Nz, e->Pz, e->en_partial.as<double>());
         k_energy_final<<<1, 1024, 0, e->stream>>>(e->en_partial.as<double>(), 1024, res);
     }
     ck(cudaGetLastError(), "energy");
@@ -1505,7 +1456,8 @@ efs_status efs_energy_noalloc(efs_engine* e, double* out) {
             return;
         }
         double* result = scratch + EN_NA_MAX_PARTIALS;
-        k_energy_ranges<<<(uint32_t)parts, 256, 0, e->stream>>>(e->vcur(), e->ccur(), e->Nx, e->Ny, e->Nz, EN_NA_CELLS, scratch);
+        k_energy_ranges<<<(uint32_t)parts, 256, 0, e->stream>>>(e->vcur(), e->ccur(), e->Nx, e->Ny, e->Nz, e->Pz, EN_NA_CELLS,
+                                                                scratch);
         k_energy_final<<<1, 1024, 0, e->stream>>>(scratch, (uint32_t)parts, result);
         ck(cudaGetLastError(), "efs_energy_noalloc");
         ck(cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "efs_energy_noalloc readback");
@@ -1529,8 +1481,8 @@ efs_status efs_flush_energy(efs_engine* e, double* out) {
 efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
     return guard(e, [&] {
         e->need_init();
-        if (v) ck(cudaMemcpyAsync(v, e->vcur(), 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read volt");
-        if (c) ck(cudaMemcpyAsync(c, e->ccur(), 3 * e->N * 4, cudaMemcpyDeviceToHost, e->stream), "read curr");
+        if (v) e->copy_fields_out(v, e->vcur());
+        if (c) e->copy_fields_out(c, e->ccur());
         e->sync("sync");
     });
 }
@@ -1538,8 +1490,8 @@ efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
 efs_status efs_set_fields(efs_engine* e, const float* v, const float* c) {
     return guard(e, [&] {
         e->need_init();
-        if (v) ck(cudaMemcpyAsync(e->vcur(), v, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write volt");
-        if (c) ck(cudaMemcpyAsync(e->ccur(), c, 3 * e->N * 4, cudaMemcpyHostToDevice, e->stream), "write curr");
+        if (v) e->copy_fields_in(e->vcur(), v);
+        if (c) e->copy_fields_in(e->ccur(), c);
         e->sync("sync");
     });
 }
@@ -1654,60 +1606,42 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
     });
 }
 
+efs_status efs_debug_set_wait(efs_engine* e, uint64_t wait_ns, uint32_t skip_plane) {
+    return guard(e, [&] {
+        if (wait_ns == 0 || wait_ns > 10000000000ull) fail(EFS_ERR_INVALID, "wait_ns must be in 1 ns .. 10 s");
+        e->wait_ns = wait_ns;
+        e->skip_plane = skip_plane;
+        e->dirty();
+    });
+}
+
 efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms) {
     return guard(e, [&] {
         e->need_init();
         if (!ms || reps == 0) fail(EFS_ERR_INVALID, "ms must be non-null and reps > 0");
         e->build_plan();
-        const Grid g = e->grid();
-        const PmlSet ps = e->pml_set();
-        const bool hp = !e->pml.empty();
-        dim3 cb(CORE_BZ, CORE_BY), cg(blocks(e->Nz, CORE_BZ), blocks(e->Ny, CORE_BY), blocks(e->Nx, CORE_TX));
-        cudaEvent_t ev[3];
+        // the fused kernel reads parity cur and writes the other one; repeated
+        // launches redo the same step, which is what is timed.  ms[0]: the fused
+        // kernel; ms[1]: the UPML passes around it
+        cudaEvent_t ev[2];
         for (auto& x : ev) ck(cudaEventCreate(&x), "event");
-        if (e->fused) {
-            // the fused kernel reads parity cur and writes the other one; repeated
-            // launches redo the same step, which is what is timed.  ms[0]: the fused
-            // kernel; ms[1]: the UPML passes around it (TMA path with UPML regions)
-            auto timed = [&](auto launch) {
-                ck(cudaEventRecord(ev[0], e->stream), "record");
-                for (uint32_t i = 0; i < reps; ++i) launch();
-                ck(cudaEventRecord(ev[1], e->stream), "record");
-                ck(cudaEventSynchronize(ev[1]), "sync");
-                float t = 0;
-                cudaEventElapsedTime(&t, ev[0], ev[1]);
-                return t / reps;
-            };
-            const int p = e->cur;
-            const float a = timed([&] { e->launch_fused(p); });
-            const float b = e->pml_split() ? timed([&] { e->launch_pml_e(p); }) + timed([&] { e->launch_pml_h(p); }) : 0.f;
-            ck(cudaGetLastError(), "fused launch");
-            for (auto& x : ev) cudaEventDestroy(x);
-            e->sync("fused timing");
-            ms[0] = a;
-            ms[1] = b;
-            return;
-        }
-        auto volt = [&] {
-            if (e->indexed) { if (hp) k_volt<true, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_volt<true, false><<<cg, cb, 0, e->stream>>>(g, ps); }
-            else { if (hp) k_volt<false, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_volt<false, false><<<cg, cb, 0, e->stream>>>(g, ps); }
+        auto timed = [&](auto launch) {
+            ck(cudaEventRecord(ev[0], e->stream), "record");
+            for (uint32_t i = 0; i < reps; ++i) launch();
+            ck(cudaEventRecord(ev[1], e->stream), "record");
+            ck(cudaEventSynchronize(ev[1]), "sync");
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[0], ev[1]);
+            return t / reps;
         };
-        auto curr = [&] {
-            if (e->indexed) { if (hp) k_curr<true, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_curr<true, false><<<cg, cb, 0, e->stream>>>(g, ps); }
-            else { if (hp) k_curr<false, true><<<cg, cb, 0, e->stream>>>(g, ps); else k_curr<false, false><<<cg, cb, 0, e->stream>>>(g, ps); }
-        };
-        ck(cudaEventRecord(ev[0], e->stream), "record");
-        for (uint32_t i = 0; i < reps; ++i) volt();
-        ck(cudaEventRecord(ev[1], e->stream), "record");
-        for (uint32_t i = 0; i < reps; ++i) curr();
-        ck(cudaEventRecord(ev[2], e->stream), "record");
-        ck(cudaEventSynchronize(ev[2]), "sync");
-        float a = 0, b = 0;
-        cudaEventElapsedTime(&a, ev[0], ev[1]);
-        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        const int p = e->cur;
+        const float a = timed([&] { e->launch_fused_tma(p); });
+        const float b = e->pml_split() ? timed([&] { e->launch_pml_e(p); }) + timed([&] { e->launch_pml_h(p); }) : 0.f;
+        ck(cudaGetLastError(), "fused launch");
         for (auto& x : ev) cudaEventDestroy(x);
-        ms[0] = a / reps;
-        ms[1] = b / reps;
+        e->sync("fused timing");
+        ms[0] = a;
+        ms[1] = b;
     });
 }
 
@@ -1716,7 +1650,7 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
         e->need_init();
         if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
         e->build_plan();
-        uint32_t k = e->fused ? 1 + (e->defer_n > 0) + 2 * e->pml_split() : 2;   // fused (+ deferred H, UPML passes) or E and H
+        uint32_t k = 1 + (e->defer_n > 0) + 2 * e->pml_split();   // fused kernel (+ deferred H, UPML passes)
         k += e->ss_on + e->ade_v.live() + e->ade_c.live() + 3 * e->mur_on + 2 * e->rlc_on;
         k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
         k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;
@@ -1728,7 +1662,7 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
 efs_status efs_device_bytes(const efs_engine* e, size_t* out) {
     if (!e || !out) return EFS_ERR_INVALID;
     size_t t = 0;
-    const DevBuf* all[] = {&e->volt, &e->curr, &e->volt_b, &e->curr_b, &e->defer_bits, &e->defer_rows, &e->defer_cells, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
+    const DevBuf* all[] = {&e->volt, &e->curr, &e->volt_b, &e->curr_b, &e->defer_cells, &e->mat, &e->table, &e->vv, &e->vi, &e->ii, &e->iv};
     for (auto* b : all) t += b->bytes;
     for (auto& r : e->pml) {
         const DevBuf* rb[] = {&r->vv, &r->vvfo, &r->vvfn, &r->ii, &r->iifo, &r->iifn, &r->vflux, &r->cflux, &r->vflux_b, &r->cflux_b};

@@ -12,10 +12,6 @@
 namespace efs {
 
 constexpr int MAX_PML = 24;     // UPML regions handled by the fused update
-constexpr int CORE_TX = 16;     // x-planes streamed per thread in the core kernels
-constexpr int CORE_BZ = 32;     // threads along z (contiguous axis)
-constexpr int CORE_BY = 8;      // threads along y
-
 struct StepState {              // device-resident, read by every per-step kernel
     uint32_t numTS;
     uint32_t ss_recording;
@@ -36,16 +32,6 @@ struct PmlRegion {
 struct PmlSet {
     int count;
     PmlRegion r[MAX_PML];
-};
-
-struct Grid {
-    uint32_t Nx, Ny, Nz, indexed;
-    size_t N, NyNz;
-    float* volt;
-    float* curr;
-    const uint32_t* mat;        // indexed mode: row per cell
-    const float* table;         //   12 floats per row
-    const float* vv; const float* vi; const float* ii; const float* iv;  // dense mode
 };
 
 __device__ __forceinline__ float upd(float vold, float cv, float ci, float curl) {
@@ -77,174 +63,6 @@ __device__ __forceinline__ uint32_t region_mask(const PmlSet& ps, const uint32_t
 __device__ __forceinline__ size_t region_p(const PmlRegion& r, uint32_t n, uint32_t x, uint32_t y, uint32_t z) {
     size_t nyz = (size_t)r.n[1] * r.n[2];
     return (size_t)n * r.n[0] * nyz + (size_t)(x - r.s[0]) * nyz + (size_t)(y - r.s[1]) * r.n[2] + (z - r.s[2]);
-}
-
-// One component of one cell through UPML pre -> core -> post
-// (src/webgpu-fdtd.mjs:239-358 around :1138/:1162).  `core` false: the core
-// update skips this cell (current loop bounds) but UPML still swaps.
-template <bool VOLT>
-__device__ __forceinline__ float pml_chain(const PmlSet& ps, uint32_t mask, uint32_t x, uint32_t y, uint32_t z, uint32_t n,
-                                           float vold, bool core, float cv, float ci, float curl) {
-    int cnt = 0, only = -1;
-    for (uint32_t m = mask; m; m &= m - 1) {
-        const int r = __ffs(m) - 1;
-        if (in_region(ps.r[r], x, y, z)) { ++cnt; only = r; }
-    }
-    if (cnt == 0) return core ? upd(vold, cv, ci, curl) : vold;
-    if (cnt == 1) {
-        const PmlRegion& R = ps.r[only];
-        size_t p = region_p(R, n, x, y, z);
-        float* flux = VOLT ? R.vflux : R.cflux;
-        const float a = VOLT ? R.vv[p] : R.ii[p];
-        const float b = VOLT ? R.vvfo[p] : R.iifo[p];
-        const float fn = VOLT ? R.vvfn[p] : R.iifn[p];
-        float fo = flux[p];
-        float fh = __fsub_rn(__fmul_rn(a, vold), __fmul_rn(b, fo));   // pre f_help
-        float v = core ? upd(fo, cv, ci, curl) : fo;                  // V = old flux, then core
-        flux[p] = v;                                                   // post: flux = V
-        return __fadd_rn(fh, __fmul_rn(fn, v));                        // V = f_help + fn*flux
-    }
-    // overlapping regions: the literal region-ordered sequence through memory
-    float v = vold;
-    for (int r = 0; r < ps.count; ++r) {
-        const PmlRegion& R = ps.r[r];
-        if (!in_region(R, x, y, z)) continue;
-        size_t p = region_p(R, n, x, y, z);
-        float* flux = VOLT ? R.vflux : R.cflux;
-        float a = VOLT ? R.vv[p] : R.ii[p], b = VOLT ? R.vvfo[p] : R.iifo[p];
-        float fo = flux[p];
-        float fh = __fsub_rn(__fmul_rn(a, v), __fmul_rn(b, fo));
-        v = fo;
-        flux[p] = fh;
-    }
-    if (core) v = upd(v, cv, ci, curl);
-    for (int r = 0; r < ps.count; ++r) {
-        const PmlRegion& R = ps.r[r];
-        if (!in_region(R, x, y, z)) continue;
-        size_t p = region_p(R, n, x, y, z);
-        float* flux = VOLT ? R.vflux : R.cflux;
-        float fn = VOLT ? R.vvfn[p] : R.iifn[p];
-        float fh = flux[p];
-        flux[p] = v;
-        v = __fadd_rn(fh, __fmul_rn(fn, v));
-    }
-    return v;
-}
-
-template <bool IDX>
-__device__ __forceinline__ void coeffs(const Grid& g, size_t c, int base, float out[6]) {
-    if (IDX) {
-        const float* t = g.table + (size_t)__ldg(g.mat + c) * 12 + base;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) out[k] = __ldg(t + k);
-    } else {
-        const float* a = base == 0 ? g.vv : g.ii;
-        const float* b = base == 0 ? g.vi : g.iv;
-        out[0] = __ldg(a + c); out[1] = __ldg(a + g.N + c); out[2] = __ldg(a + 2 * g.N + c);
-        out[3] = __ldg(b + c); out[4] = __ldg(b + g.N + c); out[5] = __ldg(b + 2 * g.N + c);
-    }
-}
-
-// E update (src/webgpu-engine.mjs:22-62 / src/webgpu-fdtd.mjs:64-106) with
-// UPML fused per cell.  Thread = one (y,z) column over CORE_TX x-planes;
-// Hy,Hz of plane x-1 stay in registers.
-template <bool IDX, bool PML>
-__global__ void __launch_bounds__(256) k_volt(const Grid g, const PmlSet ps) {
-    const uint32_t z = blockIdx.x * CORE_BZ + threadIdx.x;
-    const uint32_t y = blockIdx.y * CORE_BY + threadIdx.y;
-    if (z >= g.Nz || y >= g.Ny) return;
-    const uint32_t x0 = blockIdx.z * CORE_TX;
-    const uint32_t x1 = min(x0 + CORE_TX, g.Nx);
-    const size_t N = g.N, NyNz = g.NyNz;
-    const size_t sy = y > 0 ? g.Nz : 0, sz = z > 0 ? 1 : 0;
-    const float* __restrict__ H = g.curr;
-    float* __restrict__ V = g.volt;
-    uint32_t pmask = 0;
-    if (PML) {
-        const uint32_t lo[3] = {x0, blockIdx.y * CORE_BY, blockIdx.x * CORE_BZ};
-        const uint32_t hi[3] = {x1 - 1, lo[1] + CORE_BY - 1, lo[2] + CORE_BZ - 1};
-        pmask = region_mask(ps, lo, hi);
-    }
-    size_t c = (size_t)x0 * NyNz + (size_t)y * g.Nz + z;
-    float hy_p, hz_p;
-    if (x0 > 0) { hy_p = __ldg(H + N + c - NyNz); hz_p = __ldg(H + 2 * N + c - NyNz); }
-    else { hy_p = __ldg(H + N + c); hz_p = __ldg(H + 2 * N + c); }
-    for (uint32_t x = x0; x < x1; ++x, c += NyNz) {
-        const float hx = __ldg(H + c), hy = __ldg(H + N + c), hz = __ldg(H + 2 * N + c);
-        const float hz_ym = __ldg(H + 2 * N + c - sy), hy_zm = __ldg(H + N + c - sz);
-        const float hx_zm = __ldg(H + c - sz), hx_ym = __ldg(H + c - sy);
-        const float cx = curl4(hz, hz_ym, hy, hy_zm);
-        const float cy = curl4(hx, hx_zm, hz, hz_p);
-        const float cz = curl4(hy, hy_p, hx, hx_ym);
-        float k[6];
-        coeffs<IDX>(g, c, 0, k);
-        const float e0 = V[c], e1 = V[N + c], e2 = V[2 * N + c];
-        if (PML && pmask) {
-            V[c] = pml_chain<true>(ps, pmask, x, y, z, 0, e0, true, k[0], k[3], cx);
-            V[N + c] = pml_chain<true>(ps, pmask, x, y, z, 1, e1, true, k[1], k[4], cy);
-            V[2 * N + c] = pml_chain<true>(ps, pmask, x, y, z, 2, e2, true, k[2], k[5], cz);
-        } else {
-            V[c] = upd(e0, k[0], k[3], cx);
-            V[N + c] = upd(e1, k[1], k[4], cy);
-            V[2 * N + c] = upd(e2, k[2], k[5], cz);
-        }
-        hy_p = hy; hz_p = hz;
-    }
-}
-
-// H update (src/webgpu-engine.mjs:80-121 / src/webgpu-fdtd.mjs:113-155):
-// core over (Nx-1)(Ny-1)(Nz-1), UPML over every region cell.
-template <bool IDX, bool PML>
-__global__ void __launch_bounds__(256) k_curr(const Grid g, const PmlSet ps) {
-    const uint32_t z = blockIdx.x * CORE_BZ + threadIdx.x;
-    const uint32_t y = blockIdx.y * CORE_BY + threadIdx.y;
-    if (z >= g.Nz || y >= g.Ny) return;
-    const uint32_t x0 = blockIdx.z * CORE_TX;
-    const uint32_t x1 = min(x0 + CORE_TX, g.Nx);
-    const size_t N = g.N, NyNz = g.NyNz, Nz = g.Nz;
-    const bool yz_core = (y + 1 < g.Ny) && (z + 1 < g.Nz);
-    uint32_t pmask = 0;
-    if (PML) {
-        const uint32_t lo[3] = {x0, blockIdx.y * CORE_BY, blockIdx.x * CORE_BZ};
-        const uint32_t hi[3] = {x1 - 1, lo[1] + CORE_BY - 1, lo[2] + CORE_BZ - 1};
-        pmask = region_mask(ps, lo, hi);
-    }
-    if (!pmask && !yz_core) return;
-    const float* __restrict__ V = g.volt;
-    float* __restrict__ H = g.curr;
-    size_t c = (size_t)x0 * NyNz + (size_t)y * Nz + z;
-    float ey_c = 0.f, ez_c = 0.f;
-    if (yz_core) { ey_c = __ldg(V + N + c); ez_c = __ldg(V + 2 * N + c); }
-    for (uint32_t x = x0; x < x1; ++x, c += NyNz) {
-        const bool core = yz_core && (x + 1 < g.Nx);
-        float cx = 0.f, cy = 0.f, cz = 0.f;
-        if (core) {
-            const float ex = __ldg(V + c);
-            const float ez_yp = __ldg(V + 2 * N + c + Nz), ey_zp = __ldg(V + N + c + 1);
-            const float ex_zp = __ldg(V + c + 1), ex_yp = __ldg(V + c + Nz);
-            const float ey_xp = __ldg(V + N + c + NyNz), ez_xp = __ldg(V + 2 * N + c + NyNz);
-            cx = curl4(ez_c, ez_yp, ey_c, ey_zp);
-            cy = curl4(ex, ex_zp, ez_c, ez_xp);
-            cz = curl4(ey_c, ey_xp, ex, ex_yp);
-            ey_c = ey_xp; ez_c = ez_xp;
-        }
-        if (PML && pmask) {
-            float k[6] = {0, 0, 0, 0, 0, 0};
-            if (core) coeffs<IDX>(g, c, 6, k);
-            const float h0 = H[c], h1 = H[N + c], h2 = H[2 * N + c];
-            const float r0 = pml_chain<false>(ps, pmask, x, y, z, 0, h0, core, k[0], k[3], cx);
-            const float r1 = pml_chain<false>(ps, pmask, x, y, z, 1, h1, core, k[1], k[4], cy);
-            const float r2 = pml_chain<false>(ps, pmask, x, y, z, 2, h2, core, k[2], k[5], cz);
-            if (core || r0 != h0 || r1 != h1 || r2 != h2) { H[c] = r0; H[N + c] = r1; H[2 * N + c] = r2; }
-            // (bitwise-equal rewrites of untouched cells are skipped; NaN != NaN rewrites are harmless)
-        } else if (core) {
-            float k[6];
-            coeffs<IDX>(g, c, 6, k);
-            H[c] = upd(H[c], k[0], k[3], cx);
-            H[N + c] = upd(H[N + c], k[1], k[4], cy);
-            H[2 * N + c] = upd(H[2 * N + c], k[2], k[5], cz);
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -491,7 +309,7 @@ __global__ void k_steady_state(const float* __restrict__ V, const StepState* st,
 // Periodic / Bloch copy (src/webgpu-engine.mjs:519-584), one axis per launch.
 struct PbcDev {
     uint32_t axis, volt, src, dst, fs0, fs1, b0, b1;
-    uint32_t Nx, Ny, Nz;
+    uint32_t Nx, Ny, Nz, Pz;     // Pz: z pitch of the device layout
     float cosP, sinP;
     float* imag;       // Bloch imaginary parts of this axis, already offset
 };
@@ -504,9 +322,9 @@ __global__ void k_pbc(float* __restrict__ F, const PbcDev p) {
     if (p.axis == 0) { sp[0] = p.src; sp[1] = i0; sp[2] = i1; dp[0] = p.dst; dp[1] = i0; dp[2] = i1; }
     else if (p.axis == 1) { sp[0] = i1; sp[1] = p.src; sp[2] = i0; dp[0] = i1; dp[1] = p.dst; dp[2] = i0; }
     else { sp[0] = i0; sp[1] = i1; sp[2] = p.src; dp[0] = i0; dp[1] = i1; dp[2] = p.dst; }
-    const size_t N = (size_t)p.Nx * p.Ny * p.Nz, NyNz = (size_t)p.Ny * p.Nz;
-    const size_t s = (size_t)sp[0] * NyNz + (size_t)sp[1] * p.Nz + sp[2];
-    const size_t d = (size_t)dp[0] * NyNz + (size_t)dp[1] * p.Nz + dp[2];
+    const size_t N = (size_t)p.Nx * p.Ny * p.Pz, NyNz = (size_t)p.Ny * p.Pz;
+    const size_t s = (size_t)sp[0] * NyNz + (size_t)sp[1] * p.Pz + sp[2];
+    const size_t d = (size_t)dp[0] * NyNz + (size_t)dp[1] * p.Pz + dp[2];
     const size_t s0 = t0 * N + s, d0 = t0 * N + d, s1 = t1 * N + s, d1 = t1 * N + d;
     if (p.sinP == 0.0f) {
         F[d0] = __fmul_rn(p.cosP, F[s0]);
@@ -571,7 +389,7 @@ constexpr int NF_MAX_FREQ = 16;
 constexpr uint32_t NF_K = 16;       // steps of surface samples buffered between accumulator passes
 struct Nf2ffDev {
     uint32_t np, nf, maxTS, window;
-    uint32_t Nx, Ny, Nz;
+    uint32_t Nx, Ny, Nz, Pz;        // Pz: z pitch of the device layout
     uint32_t off[6];
     const uint32_t* pts;
     const float* el;
@@ -584,8 +402,8 @@ struct Nf2ffDev {
 __device__ __forceinline__ void nf2ff_fields(const float* __restrict__ V, const float* __restrict__ C, const Nf2ffDev& d,
                                              uint32_t pid, float E[3], float Hh[3]) {
     const uint32_t ix = d.pts[3 * pid], iy = d.pts[3 * pid + 1], iz = d.pts[3 * pid + 2];
-    const size_t Ny = d.Ny, Nz = d.Nz, N = (size_t)d.Nx * Ny * Nz, NyNz = Ny * Nz;
-    auto fi = [&](uint32_t x, uint32_t y, uint32_t z) { return (size_t)x * NyNz + (size_t)y * Nz + z; };
+    const size_t Ny = d.Ny, Pz = d.Pz, N = (size_t)d.Nx * Ny * Pz, NyNz = Ny * Pz;
+    auto fi = [&](uint32_t x, uint32_t y, uint32_t z) { return (size_t)x * NyNz + (size_t)y * Pz + z; };
     const size_t base = fi(ix, iy, iz);
     const bool atB = (ix >= d.Nx - 1) || (iy >= d.Ny - 1) || (iz >= d.Nz - 1);
     E[0] = E[1] = E[2] = 0.f;
@@ -600,7 +418,7 @@ __device__ __forceinline__ void nf2ff_fields(const float* __restrict__ V, const 
         E[2] = __fdiv_rn(a, __fmul_rn(4.0f, elZ));
     }
     const uint32_t pos[3] = {ix, iy, iz}, lim[3] = {d.Nx, d.Ny, d.Nz};
-    const size_t step[3] = {NyNz, Nz, 1};
+    const size_t step[3] = {NyNz, Pz, 1};
     for (int n = 0; n < 3; ++n) {
         const float d0 = d.el[d.off[3 + n] + pos[n]];
         if (!(d0 > 0.0f)) continue;
@@ -713,13 +531,13 @@ __global__ void __launch_bounds__(256) k_nf2ff_flush(const StepState* st, uint32
 // 3071-3145), block-then-warp reduction with f64 block partials.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_energy(const float* __restrict__ V, const float* __restrict__ C, uint32_t Nx,
-                                                uint32_t Ny, uint32_t Nz, double* partial) {
-    const size_t N = (size_t)Nx * Ny * Nz, inner = (size_t)(Nx - 1) * (Ny - 1) * (Nz - 1);
+                                                uint32_t Ny, uint32_t Nz, uint32_t Pz, double* partial) {
+    const size_t N = (size_t)Nx * Ny * Pz, inner = (size_t)(Nx - 1) * (Ny - 1) * (Nz - 1);
     const size_t iNz = Nz - 1, iNyNz = (size_t)(Ny - 1) * (Nz - 1);
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < inner; i += (size_t)gridDim.x * blockDim.x) {
         const size_t x = i / iNyNz, r = i - x * iNyNz, y = r / iNz, z = r - y * iNz;
-        const size_t c = x * Ny * Nz + y * Nz + z;
+        const size_t c = (x * Ny + y) * Pz + z;
         float s = 0.f;
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
@@ -757,14 +575,15 @@ __global__ void k_energy_final(const double* partial, uint32_t n, double* out) {
 // partial[b], so the number of partial sums grows with the grid and a fixed
 // scratch array bounds the grid it accepts.  Same per-cell f32 arithmetic.
 __global__ void __launch_bounds__(256) k_energy_ranges(const float* __restrict__ V, const float* __restrict__ C, uint32_t Nx,
-                                                       uint32_t Ny, uint32_t Nz, uint64_t cells, double* partial) {
-    const size_t N = (size_t)Nx * Ny * Nz, inner = (size_t)(Nx - 1) * (Ny - 1) * (Nz - 1);
+                                                       uint32_t Ny, uint32_t Nz, uint32_t Pz, uint64_t cells,
+                                                       double* partial) {
+    const size_t N = (size_t)Nx * Ny * Pz, inner = (size_t)(Nx - 1) * (Ny - 1) * (Nz - 1);
     const size_t iNz = Nz - 1, iNyNz = (size_t)(Ny - 1) * (Nz - 1);
     const size_t lo = (size_t)blockIdx.x * cells, hi = min(lo + cells, inner);
     double acc = 0.0;
     for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const size_t x = i / iNyNz, r = i - x * iNyNz, y = r / iNz, z = r - y * iNz;
-        const size_t c = x * Ny * Nz + y * Nz + z;
+        const size_t c = (x * Ny + y) * Pz + z;
         float s = 0.f;
 #pragma unroll
         for (int n = 0; n < 3; ++n) {

@@ -1,5 +1,4 @@
-// efs_tma.cuh — TMA-fed single-pass E+H update (the engine's default core path
-// when Nz is a multiple of 4).
+// efs_tma.cuh — TMA-fed single-pass E+H update (the engine's core path).
 //
 // A CTA owns a tile of TT_Y rows (y) x TT_Z columns (z) and streams the
 // x-planes of one x-chunk through a TT_S-stage shared-memory pipeline: one
@@ -7,7 +6,11 @@
 // low halos, E_old and the material rows, each a box of the tile plus halos)
 // completing on the stage's mbarrier, TT_S-1 planes ahead of the plane being
 // computed.  The loads run on the copy engine, so the bytes in flight per SM
-// do not depend on how many warps are resident.
+// do not depend on how many warps are resident.  The tensor maps span the
+// grid's Nz x Ny x Nx cells over the padded device layout (row pitch Pz, a
+// multiple of 4 floats, so every global stride is a multiple of 16 bytes):
+// box columns at z >= Nz lie outside the map and are zero-filled, so pad
+// cells are never loaded.
 //
 // At plane x (local index k = x - xs) the CTA
 //   1. computes E_new(x) on the tile plus its high halo row and column from
@@ -29,9 +32,11 @@
 // rewritten by sparse post-update operations are written here provisionally
 // and rewritten afterwards by k_deferred_h, which recomputes them from H_old.
 //
-// Every mbarrier wait is bounded (about one second of %globaltimer); a wait
-// that runs out sets bit 0 of *g.status, the CTA drains its loads in flight
-// (bounded again) and returns, and the host reports EFS_ERR_TIMEOUT.
+// Every mbarrier wait is bounded (g.wait_ns of %globaltimer, about one
+// second); a wait that runs out sets bit 0 of *g.status, the CTA drains its
+// loads in flight (bounded again) and returns, and the host reports
+// EFS_ERR_TIMEOUT.  A diagnostic knob (g.skip_plane) leaves one plane's loads
+// unissued so that tests can make a wait run out without any fault.
 #pragma once
 #include "efs_fused.cuh"
 #include <cuda.h>
@@ -146,8 +151,8 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
     const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;           // last plane whose E this CTA computes
     const int nk = (int)(xl - xs) + 1;                       // planes streamed
-    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Ny = g.Ny, Nz = g.Nz;   // 3*N < 2^32
-    constexpr uint64_t WAIT_NS = 1000000000ull;
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Ny = g.Ny, Nz = g.Nz, Pz = g.Pz;   // 3*N < 2^32
+    const uint64_t WAIT_NS = g.wait_ns;
     constexpr int HPL = TT_HY * TT_HZ;                       // one component of a staged H box
     constexpr int EPL = TT_EY * TT_EZ;                       // one component of a staged E box / E_new plane
 
@@ -164,7 +169,7 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
         sy[q] = y0 + sr[q]; sz[q] = z0 + sc[q];
         sin[q] = sy[q] < Ny && sz[q] < Nz && (q < 2 || has2);
         core[q] = sy[q] + 1 < Ny && sz[q] + 1 < Nz;
-        off[q] = sy[q] * Nz + sz[q];                         // offset inside a plane (used when sin)
+        off[q] = sy[q] * Pz + sz[q];                         // offset inside a plane (used when sin)
         hi[q] = (sr[q] + 1) * TT_HZ + sc[q] + 4;             // index in a staged H component
         ei[q] = sr[q] * TT_EZ + sc[q];                       // index in a staged E component / E_new plane
         dym[q] = sy[q] == 0 ? 0 : TT_HZ;                     // y-1 neighbour (self at y = 0)
@@ -185,7 +190,8 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
     int issued = 0;                                          // planes issued (thread 0's count)
     if (threadIdx.x == 0)
         for (; issued < TT_S && issued < nk; ++issued)
-            tt_issue<IDX>(S, (int)((K + issued) % TT_S), tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);
+            if (xs + issued != g.skip_plane)
+                tt_issue<IDX>(S, (int)((K + issued) % TT_S), tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);
 
     // H_old(xs-1) of the E cells (y, z components); at xs = 0 the x-1 neighbour is plane 0 itself
     float hp[3][3];
@@ -270,7 +276,8 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
         timed_out = __syncthreads_or(!ok) != 0;
         if (timed_out) break;
         if (threadIdx.x == 0 && issued < nk) {
-            tt_issue<IDX>(S, s, tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);   // stage of plane k+TT_S
+            if (xs + issued != g.skip_plane)
+                tt_issue<IDX>(S, s, tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);   // stage of plane k+TT_S
             ++issued;
         }
         // ---- H_new(x-1) of the owned cells
@@ -318,7 +325,8 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
         if (threadIdx.x == 0) {
             atomicOr(g.status, 1u);
             for (int j = k; j < issued; ++j)                       // drain the loads still in flight
-                (void)mbar_wait_bounded(smem_u32(&S.full[(K + j) % TT_S]), ((K + j) / TT_S) & 1u, WAIT_NS);
+                if (xs + j != g.skip_plane)
+                    (void)mbar_wait_bounded(smem_u32(&S.full[(K + j) % TT_S]), ((K + j) / TT_S) & 1u, WAIT_NS);
         }
         return false;
     }
@@ -450,9 +458,9 @@ __device__ __forceinline__ void pml_e_body(const FusedGrid& g, const PmlSet& ps,
     int r;
     uint32_t x, y, z0, cnt;
     if (!pml_item(ps, i, r, x, y, z0, cnt)) return;
-    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;
-    const uint32_t c0 = x * NyNz + y * Nz + z0;
-    const uint32_t dx = x > 0 ? NyNz : 0u, dy = y > 0 ? Nz : 0u;      // x-1 / y-1 neighbour (self at index 0)
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Pz = g.Pz;
+    const uint32_t c0 = x * NyNz + y * Pz + z0;
+    const uint32_t dx = x > 0 ? NyNz : 0u, dy = y > 0 ? Pz : 0u;      // x-1 / y-1 neighbour (self at index 0)
     const float* H = g.H0;
     const PmlRegion& R = ps.r[r];
     uint32_t mask[PML_ZC], m[PML_ZC];
@@ -512,8 +520,8 @@ __device__ __forceinline__ void pml_h_body(const FusedGrid& g, const PmlSet& ps,
     int r;
     uint32_t x, y, z0, cnt;
     if (!pml_item(ps, i, r, x, y, z0, cnt)) return;
-    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Nz = g.Nz;
-    const uint32_t c0 = x * NyNz + y * Nz + z0;
+    const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Pz = g.Pz;
+    const uint32_t c0 = x * NyNz + y * Pz + z0;
     const float* V = g.V1;
     const PmlRegion& R = ps.r[r];
     uint32_t mask[PML_ZC], m[PML_ZC];
@@ -528,12 +536,12 @@ __device__ __forceinline__ void pml_h_body(const FusedGrid& g, const PmlSet& ps,
         core[j] = core_xy && (z0 + j + 1 < g.Nz);
         if (core[j]) {
             ev[j][0] = V[c]; ev[j][1] = V[N + c]; ev[j][2] = V[2 * N + c];
-            ev[j][3] = V[2 * N + c + Nz];      // ez(y+1)
+            ev[j][3] = V[2 * N + c + Pz];      // ez(y+1)
             ev[j][4] = V[N + c + 1];           // ey(z+1)
             ev[j][5] = V[c + 1];               // ex(z+1)
             ev[j][6] = V[2 * N + c + NyNz];    // ez(x+1)
             ev[j][7] = V[N + c + NyNz];        // ey(x+1)
-            ev[j][8] = V[c + Nz];              // ex(y+1)
+            ev[j][8] = V[c + Pz];              // ex(y+1)
             m[j] = IDX ? __ldg(g.mat + c) : 0u;
         }
         ho[j][0] = g.H0[c]; ho[j][1] = g.H0[N + c]; ho[j][2] = g.H0[2 * N + c];

@@ -431,8 +431,13 @@ class CudaEngine:
         self._ck(self._lib.efs_device_bytes(self._h, C.byref(v)))
         return v.value
 
+    def debugSetWait(self, wait_ns=1_000_000_000, skip_plane=None):
+        """Diagnostics (efs_debug_set_wait): limit of the fused kernel's bounded
+        waits, and an x-plane whose loads are never issued (None: none)."""
+        self._ck(self._lib.efs_debug_set_wait(self._h, int(wait_ns), 0xFFFFFFFF if skip_plane is None else int(skip_plane)))
+
     def timeCore(self, reps=10):
-        """Mean device ms per launch of the core kernels [E, H] (advances the fields)."""
+        """Mean device ms per launch of [the fused kernel, the UPML passes] (advances the fields)."""
         ms = np.zeros(2, np.float32)
         self._ck(self._lib.efs_time_core(self._h, int(reps), _p(ms, C.c_float)))
         return [float(ms[0]), float(ms[1])]

@@ -43,7 +43,7 @@ class Request:
 def estimate_bytes(job):
     """Device bytes a job will hold once configured (upper estimate for admission)."""
     g = job["grid"]
-    n = g[0] * g[1] * g[2]
+    n = g[0] * g[1] * ((g[2] + 3) // 4 * 4)                     # device cells: z rows padded to 4 floats
     b = n * (4 * 3 * 4 + 4)                                     # E, H in two parities + material index
     if job.get("mur"):
         b += len(job["mur"]["coeff_nyP"]) * 2 * 48
@@ -53,7 +53,7 @@ def estimate_bytes(job):
     if job.get("nf2ff"):
         nf = job["nf2ff"]
         b += nf["numPoints"] * (len(nf["omegas"]) * 48 + 16 * 24 + 32)
-    b += n // 8                                                 # deferred-H bitmask and lists
+    b += n // 8                                                 # deferred-H cell list
     return b + (8 << 20)
 
 

@@ -377,8 +377,7 @@ def _stub_filter_one(args):
 
 def stub_filters(count=64, seed=3, delta=0.2e-3, steps=15000, workers=None):
     """The batched sweep workload: `count` microstrip stub filters with
-    per-axis line counts ~ U[60, 180] (numpy default_rng(seed); Nz rounded up
-    to a multiple of 4, which the TMA-fed kernel needs), uniform `delta` mesh
+    per-axis line counts ~ U[60, 180] (numpy default_rng(seed)), uniform `delta` mesh
     (so every instance shares dT and the excitation signal).  PEC ground on
     the z = 0 face, a 0.8 mm substrate eps_r = 3.66, a 1.8 mm PEC trace along
     x with a stub along +y of seeded length U[8, 20] mm (cut to the room the
@@ -387,7 +386,6 @@ def stub_filters(count=64, seed=3, delta=0.2e-3, steps=15000, workers=None):
     current probes at both ports, Mur ABC on the other five faces."""
     rng = np.random.default_rng(seed)
     sizes = rng.integers(60, 181, (count, 3))
-    sizes[:, 2] = (sizes[:, 2] + 3) // 4 * 4
     stub_mm = rng.uniform(8e-3, 20e-3, count)
     sub = int(round(0.8e-3 / delta))
     w = int(round(1.8e-3 / delta))
@@ -434,14 +432,14 @@ def _served_tfsf_one(args):
 
 def served_template(kind, side, delta=0.5e-3, steps=25000):
     """Inputs of one request of the served stream, for a cubic grid of
-    `side` lines (Nz rounded up to a multiple of 4): kind "port" is a stub
+    `side` lines: kind "port" is a stub
     filter (two 50 ohm lumped ports, Mur on five faces, Gaussian 0-7 GHz at
     port 1, probes at both ports); kind "tfsf" is a vacuum cube holding a
     dielectric box (eps_r = 4), a TFSF Gaussian plane wave (normal incidence,
     10 GHz +- 5 GHz) on the box 6 cells in, NF2FF on the box 3 cells in at 2
     frequencies, Mur on all six faces.  The signal covers `steps` timesteps;
     a request runs its own step count on these inputs."""
-    nz = (side + 3) // 4 * 4
+    nz = side
     if kind == "port":
         sub, w = 4, 9
         d = 0.2e-3                                   # port jobs keep the stub filters' 0.2 mm cells

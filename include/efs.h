@@ -266,13 +266,22 @@ efs_status efs_device_bytes(const efs_engine* e, size_t* out);
  * engine class itself. */
 efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* out, size_t cap, size_t* count);
 
-/* Diagnostics: launch the engine's core field-update kernel(s) `reps` times
- * on its stream and return the mean device time per launch (CUDA events).
- * Separate sweeps: ms[0] = E update, ms[1] = H update.  Fused path: ms[0] =
- * the fused E+H kernel, ms[1] = the UPML-cell passes around it (0 without
- * UPML regions or off the TMA-fed kernel).  Advances the fields; meant for
- * benchmarks only.  No counterpart in the reference. */
+/* Diagnostics: launch the engine's core field-update kernels `reps` times
+ * on its stream and return the mean device time per launch (CUDA events):
+ * ms[0] = the fused E+H kernel, ms[1] = the UPML-cell passes around it (0
+ * without UPML regions).  Advances the fields; meant for benchmarks only.
+ * No counterpart in the reference. */
 efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms);
+
+/* Diagnostics for failure detection: the limit of every bounded wait in the
+ * fused kernel (default 1 s = 1e9 ns; 1 ns .. 10 s accepted) and an x-plane
+ * whose loads the kernel never issues (~0u = none, the default).  With a
+ * plane skipped, every CTA that streams it gives up after wait_ns, drains
+ * its other loads and returns; the next synchronising call returns
+ * EFS_ERR_TIMEOUT and the engine's fields are then undefined.  Nothing
+ * faults or hangs: the wait gives up.  The reference only logs a lost device
+ * (src/webgpu-engine.mjs:1129-1131). */
+efs_status efs_debug_set_wait(efs_engine* e, uint64_t wait_ns, uint32_t skip_plane);
 
 /* Diagnostics: kernel launches one timestep enqueues with the current
  * configuration (a captured batch of n steps adds one counter update and,

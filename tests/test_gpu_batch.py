@@ -32,8 +32,8 @@ def member(cls, kind, indexed):
     g = cls()
     assert g.initGPU()
     r = np.random.default_rng(100 + kind)
-    if kind == 0:                         # Mur + lumped-port style excitation + probe ring
-        N = (20, 18, 24)
+    if kind == 0:                         # Mur + lumped-port style excitation + probe ring; Nz odd (padded rows)
+        N = (20, 18, 23)
         g.init(N, coeffs(N, 1, indexed))
         g.configureMur(mur_faces(N, 2))
         sig = np.sin(np.arange(60) * 0.3).astype(np.float32)
@@ -62,11 +62,11 @@ def member(cls, kind, indexed):
             job = dict(job, coefficients=dict(vv=vv, vi=vi, ii=ii, iv=iv))
         from efs_b200.workloads import configure
         configure(g, job)
-    else:                                 # small grid, excitation only
-        N = (9, 11, 8)
+    else:                                 # small grid, excitation only; Nz = 7 (padded rows)
+        N = (9, 11, 7)
         g.init(N, coeffs(N, 7, indexed))
         g.configureExcitation(dict(signal=np.ones(5, np.float32), delay=[1], amp=[0.7], dir=[1],
-                                   pos=[4 * 88 + 5 * 8 + 3], period=3))
+                                   pos=[4 * 77 + 5 * 7 + 3], period=3))
     t = 3 * N[0] * N[1] * N[2]
     g.uploadFields(r.standard_normal(t).astype(np.float32), r.standard_normal(t).astype(np.float32))
     return g
@@ -152,9 +152,10 @@ def test_batch_rejects_unsupported_members(cuda_engine_cls):
     g = member(cuda_engine_cls, 2, True)
     odd = cuda_engine_cls()
     assert odd.initGPU()
-    N = (6, 6, 7)                              # Nz not a multiple of 4: no TMA path
+    N = (6, 6, 7)
     odd.init(N, coeffs(N, 9, True))
-    with pytest.raises(EfsError):
+    odd.configureRLC(dict(elements=[dict(field_idx=idx(0, 2, 2, 2, *N), direction=2, type_flag=0, i2v=0.1, ilv=0.2)]))
+    with pytest.raises(EfsError):              # lumped RLC members are not batched
         CudaBatch([g, odd])
     with pytest.raises(EfsError):
         CudaBatch([g, g])
