@@ -55,6 +55,7 @@ SIGNATURES = {
     "efs_configure_mur": (C.c_int, [vp, f32p, u32p, u32p, u32]),
     "efs_configure_tfsf": (C.c_int, [vp, f32p, u32, u32, C.POINTER(TfsfPoint), u32, C.POINTER(TfsfPoint), u32]),
     "efs_configure_ade": (C.c_int, [vp, u32, C.POINTER(AdeOrder)]),
+    "efs_configure_ade_apply": (C.c_int, [vp, C.c_int]),
     "efs_configure_rlc": (C.c_int, [vp, u32, C.POINTER(RlcElement)]),
     "efs_configure_pbc": (C.c_int, [vp, u32, u32p, f64p]),
     "efs_configure_steady_state": (C.c_int, [vp, u32p, u32, u32, C.c_float]),

@@ -83,6 +83,13 @@ struct OpAde {
     const float* F; AdeDev a;
     __device__ void run(uint32_t blk, uint32_t, uint32_t, uint32_t) const { ade_body(F, a, blk * blockDim.x + threadIdx.x); }
 };
+struct OpAdeApply {
+    float* F; AdeApplyDev a; uint32_t runs;
+    __device__ void run(uint32_t blk, uint32_t, uint32_t, uint32_t) const {
+        if (runs) ade_apply_runs_body(F, a, blk * blockDim.x + threadIdx.x);
+        else ade_apply_grouped_body(F, a, blk * blockDim.x + threadIdx.x);
+    }
+};
 struct OpRing {
     const float* V; const float* C; const StepState* st; RingDev r;
     __device__ void run(uint32_t blk, uint32_t k, uint32_t, uint32_t) const {
@@ -158,7 +165,8 @@ struct efs_batch {
     uint32_t phase = 0;
     DevBuf members[2], tiles[2];               // tiles[1]: material-index members, tiles[0]: dense members
     uint32_t ntiles[2] = {0, 0};
-    SegLaunch mur_pre[2], mur_post[2], mur_apply[2], exc[2], tfsf_v[2], tfsf_c[2], ade_v[2], ade_c[2], ring[2], nf_sample[2], nf_flush[2],
+    SegLaunch mur_pre[2], mur_post[2], mur_apply[2], exc[2], tfsf_v[2], tfsf_c[2], ade_v[2], ade_c[2], ade_apply_v[2], ade_apply_c[2],
+        ring[2], nf_sample[2], nf_flush[2],
         deferred_i[2], deferred_d[2], pml_e_i[2], pml_e_d[2], pml_h_i[2], pml_h_d[2], advance;   // _i / _d: index / dense members
     bool any_nf = false;
     std::map<uint32_t, cudaGraphExec_t> graphs;
@@ -228,6 +236,7 @@ struct efs_batch {
             std::vector<std::pair<uint32_t, OpPoints<0>>> vexc;
             std::vector<std::pair<uint32_t, OpPoints<1>>> vtv, vtc;
             std::vector<std::pair<uint32_t, OpAde>> vav, vac;
+            std::vector<std::pair<uint32_t, OpAdeApply>> vpv, vpc;
             std::vector<std::pair<uint32_t, OpRing>> vring;
             std::vector<std::pair<uint32_t, OpNfSample>> vns;
             std::vector<std::pair<uint32_t, OpNfFlush>> vnf;
@@ -277,6 +286,13 @@ struct efs_batch {
                     vav.push_back({(e->ade_v.n + ADE_V - 1) / ADE_V, OpAde{V, e->ade_dev(e->ade_v, e->vflux_ptrs[p].as<const float*>())}});
                 if (e->ade_c.live())
                     vac.push_back({(e->ade_c.n + ADE_V - 1) / ADE_V, OpAde{e->cbuf(p), e->ade_dev(e->ade_c, e->cflux_ptrs[p].as<const float*>())}});
+                // ADE apply step: threads of ADE_V entries (runs form) or one per location (grouped form)
+                for (int side = 0; side < 2; ++side) {
+                    const efs_engine::AdeSide& as = side == 0 ? e->ade_v : e->ade_c;
+                    if (!e->ade_apply || !as.live()) continue;
+                    const uint32_t thr = as.app_runs ? (as.app_n + ADE_V - 1) / ADE_V : as.app_n;
+                    (side == 0 ? vpv : vpc).push_back({thr, OpAdeApply{side == 0 ? V1 : C1, e->ade_apply_dev(as), as.app_runs ? 1u : 0u}});
+                }
                 if (e->ring_on) vring.push_back({e->ring_n, OpRing{V1, C1, st, e->ring_dev()}});
                 if (e->nf_on) {
                     vns.push_back({e->nf.np, OpNfSample{V1, C1, e->nf}});
@@ -307,6 +323,8 @@ struct efs_batch {
             build_seg(tfsf_c[s], vtc);
             build_seg(ade_v[s], vav);
             build_seg(ade_c[s], vac);
+            build_seg(ade_apply_v[s], vpv);
+            build_seg(ade_apply_c[s], vpc);
             build_seg(ring[s], vring);
             build_seg(nf_sample[s], vns);
             build_seg(nf_flush[s], vnf);
@@ -359,9 +377,11 @@ struct efs_batch {
         launch_seg<OpMurPost>(mur_post[s], k);
         launch_seg<OpPoints<0>>(exc[s], k);
         launch_seg<OpMurApply>(mur_apply[s], k);
+        launch_seg<OpAdeApply>(ade_apply_v[s], k);
         launch_seg<OpDeferred<true>>(deferred_i[s], k);
         launch_seg<OpDeferred<false>>(deferred_d[s], k);
         launch_seg<OpPoints<1>>(tfsf_c[s], k);
+        launch_seg<OpAdeApply>(ade_apply_c[s], k);
         if (any_nf) {
             const uint32_t j = k % NF_K;
             launch_seg<OpNfSample>(nf_sample[s], k, j);

@@ -181,6 +181,11 @@ struct efs_engine {
         std::vector<uint32_t> h_coef;    // per entry: coefficient tuple id, bit 31 set for Lorentz
         DevBuf runs, grp_run, coef, state, lor;
         uint32_t n = 0;
+        // apply step (efs_configure_ade_apply): runs over the field locations
+        // when no two entries share one, else entries grouped by location
+        bool app_runs = true;
+        uint32_t app_n = 0;                          // entries (runs form) or locations (grouped form)
+        DevBuf app_run, app_grp, app_target, app_off, app_perm;
         // A side whose coefficients are all zero keeps its state at +0 while
         // the fields stay finite (0*x + 0*y rounds to +0), so its kernel is
         // skipped until a restored state may have put other values there.
@@ -188,6 +193,7 @@ struct efs_engine {
         bool live() const { return n && !(zero && clean); }
     };
     AdeSide ade_v, ade_c;
+    bool ade_apply = false;      // opt-in: subtract the ADE state from E / H after the update (no reference counterpart)
 
     // RLC
     bool rlc_on = false;
@@ -394,8 +400,52 @@ struct efs_engine {
             runs.push_back(AdeRun{s->n, 0, 0, 0});      // sentinel: ends the last run
             upload(s->runs, runs);
             upload(s->grp_run, qr);
+            if (ade_apply) build_ade_apply(*s);
         }
         plan_dirty = false;
+    }
+
+    // Apply-step plan of one ADE side: runs over consecutive field locations
+    // when every entry has its own location, else groups per location.
+    void build_ade_apply(AdeSide& s) {
+        std::vector<uint64_t> seen((3 * Nd + 63) / 64, 0);   // one bit per device field location
+        s.app_runs = true;
+        for (uint32_t f : s.h_field) {
+            const uint64_t bit = 1ull << (f & 63);
+            if (seen[f >> 6] & bit) { s.app_runs = false; break; }
+            seen[f >> 6] |= bit;
+        }
+        if (s.app_runs) {
+            std::vector<AdeRun> runs;
+            for (uint32_t i = 0; i < s.n; ++i)
+                if (i == 0 || s.h_field[i] != s.h_field[i - 1] + 1) runs.push_back(AdeRun{i, 0, s.h_field[i], 0});
+            const uint32_t nq = (s.n + ADE_V - 1) / ADE_V;
+            std::vector<uint32_t> qr(nq);
+            size_t r = 0;
+            for (uint32_t q = 0; q < nq; ++q) {
+                while (r + 1 < runs.size() && runs[r + 1].entry <= q * ADE_V) ++r;
+                qr[q] = (uint32_t)r;
+            }
+            runs.push_back(AdeRun{s.n, 0, 0, 0});
+            upload(s.app_run, runs);
+            upload(s.app_grp, qr);
+            s.app_n = s.n;
+        } else {
+            std::vector<uint32_t> ut, off, perm;
+            group_by(s.h_field, ut, off, perm);
+            upload(s.app_target, ut);
+            upload(s.app_off, off);
+            upload(s.app_perm, perm);
+            s.app_n = (uint32_t)ut.size();
+        }
+    }
+    AdeApplyDev ade_apply_dev(const AdeSide& s) const {
+        return AdeApplyDev{s.app_n, s.app_run.as<AdeRun>(), s.app_grp.as<uint32_t>(), s.app_target.as<uint32_t>(),
+                           s.app_off.as<uint32_t>(), s.app_perm.as<uint32_t>(), s.state.as<float>()};
+    }
+    void launch_ade_apply(const AdeSide& s, float* F) {
+        if (s.app_runs) k_ade_apply_runs<<<blocks(s.app_n, ADE_BLOCK), ADE_T, 0, stream>>>(F, ade_apply_dev(s));
+        else k_ade_apply_grouped<<<blocks(s.app_n, 256), 256, 0, stream>>>(F, ade_apply_dev(s));
     }
 
     // H cells whose curl reads an E value rewritten by a sparse post-update
@@ -409,6 +459,7 @@ struct efs_engine {
         if (exc_on) add(h_exc_targets);
         if (mur_on) add(h_mur_apply);
         if (rlc_on) add(h_rlc_series);
+        if (ade_apply && ade_v.live()) add(ade_v.h_field);
         const uint32_t nl[3] = {Nx, Ny, Nz};
         if (pbc_on)
             for (auto& a : pbc_axes) {
@@ -491,6 +542,7 @@ struct efs_engine {
         }
         if (mur_on) k_mur_apply<<<blocks(mur_napply, T), T, 0, stream>>>(V1, md);
         if (rlc_on) k_rlc_apply<<<blocks(rlc_groups, T), T, 0, stream>>>(V1, rd);
+        if (ade_apply && ade_v.live()) launch_ade_apply(ade_v, V1);
         if (defer_n) {
             const FusedGrid fg = fused_grid(p);
             const uint32_t* cells = defer_cells.as<uint32_t>();
@@ -500,6 +552,7 @@ struct efs_engine {
         // --- post-current (on the updated H) ---
         if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C1, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
         if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, false, C1);
+        if (ade_apply && ade_c.live()) launch_ade_apply(ade_c, C1);
         // --- after the step ---
         if (nf_on) {
             // surface samples of this step; the accumulators take every NF_K steps
@@ -707,6 +760,7 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     e->pml.clear();
     e->exc_on = e->mur_on = e->tfsf_on = e->ade_on = e->rlc_on = e->ss_on = e->pbc_on = e->ring_on = e->nf_on = false;
     e->ade_v = efs_engine::AdeSide(); e->ade_c = efs_engine::AdeSide();
+    e->ade_apply = false;
     e->gd_n = 0;
     e->Nx = dims[0]; e->Ny = dims[1]; e->Nz = dims[2]; e->N = N; e->Pz = Pz; e->Nd = Nd;
     e->h_exc_targets.clear(); e->h_tfsf_v_targets.clear(); e->h_mur_apply.clear(); e->h_rlc_series.clear();
@@ -1082,6 +1136,14 @@ efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order*
             e->alloc(s.state, (size_t)s.n * 4); e->alloc(s.lor, (size_t)s.n * 4);
         }
         e->ade_on = count > 0;
+        e->dirty();
+    });
+}
+
+efs_status efs_configure_ade_apply(efs_engine* e, int on) {
+    return guard(e, [&] {
+        e->need_init();
+        e->ade_apply = on != 0;
         e->dirty();
     });
 }
@@ -1652,6 +1714,7 @@ efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
         e->build_plan();
         uint32_t k = 1 + (e->defer_n > 0) + 2 * e->pml_split();   // fused kernel (+ deferred H, UPML passes)
         k += e->ss_on + e->ade_v.live() + e->ade_c.live() + 3 * e->mur_on + 2 * e->rlc_on;
+        if (e->ade_apply) k += e->ade_v.live() + e->ade_c.live();
         k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
         k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;
         k += e->nf_on + e->ring_on;

@@ -245,6 +245,64 @@ __global__ void __launch_bounds__(ADE_T) k_ade(const float* __restrict__ F, cons
     ade_body(F, a, blockIdx.x * ADE_T + threadIdx.x);
 }
 
+// Opt-in ADE apply step (the reference updates the state only; openEMS's
+// Apply2Voltages / Apply2Current subtract it): after the apply-to-voltages
+// phase (E side) or the post-current phase (H side), F -= state for every
+// entry, in configuration order.  When no two entries share a field
+// location, the entries are stored as runs over consecutive locations (as
+// AdeRun with sel 0) and a thread takes ADE_V entries; otherwise entries are
+// grouped by location (ascending) and a thread applies one location's
+// entries in configuration order.
+struct AdeApplyDev {
+    uint32_t n;                     // entries (runs form) or locations (grouped form)
+    const AdeRun* runs;             // runs form: + sentinel {n, 0, 0, 0}
+    const uint32_t* grp_run;        // runs form: run of entry q*ADE_V
+    const uint32_t* target;         // grouped form: location per group
+    const uint32_t* off;            // grouped form: entries perm[off[g] .. off[g+1]) of group g
+    const uint32_t* perm;
+    const float* state;
+};
+__device__ __forceinline__ void ade_apply_runs_body(float* __restrict__ F, const AdeApplyDev& a, uint32_t q) {
+    const uint32_t i0 = q * ADE_V;
+    if (i0 >= a.n) return;
+    const uint32_t cnt = min(ADE_V, a.n - i0);
+    float st[ADE_V];
+    if (cnt == ADE_V) {
+#pragma unroll
+        for (uint32_t h = 0; h < ADE_V / 4; ++h) {
+            const float4 v = *reinterpret_cast<const float4*>(a.state + i0 + 4 * h);
+            st[4 * h] = v.x; st[4 * h + 1] = v.y; st[4 * h + 2] = v.z; st[4 * h + 3] = v.w;
+        }
+    } else {
+        for (uint32_t k = 0; k < ADE_V; ++k) st[k] = k < cnt ? a.state[i0 + k] : 0.f;
+    }
+    uint32_t lo = __ldg(a.grp_run + q);
+    AdeRun r = a.runs[lo];
+    uint32_t next = a.runs[lo + 1].entry;
+#pragma unroll
+    for (uint32_t k = 0; k < ADE_V; ++k) {
+        if (k < cnt) {
+            const uint32_t i = i0 + k;
+            while (i >= next) { ++lo; r = a.runs[lo]; next = a.runs[lo + 1].entry; }
+            const uint32_t t = r.idx + (i - r.entry);
+            F[t] = __fsub_rn(F[t], st[k]);
+        }
+    }
+}
+__device__ __forceinline__ void ade_apply_grouped_body(float* __restrict__ F, const AdeApplyDev& a, uint32_t g) {
+    if (g >= a.n) return;
+    const uint32_t t = a.target[g];
+    float v = F[t];
+    for (uint32_t e = a.off[g]; e < a.off[g + 1]; ++e) v = __fsub_rn(v, a.state[a.perm[e]]);
+    F[t] = v;
+}
+__global__ void __launch_bounds__(ADE_T) k_ade_apply_runs(float* __restrict__ F, const AdeApplyDev a) {
+    ade_apply_runs_body(F, a, blockIdx.x * ADE_T + threadIdx.x);
+}
+__global__ void __launch_bounds__(256) k_ade_apply_grouped(float* __restrict__ F, const AdeApplyDev a) {
+    ade_apply_grouped_body(F, a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // Lumped RLC (src/webgpu-fdtd.mjs:775-863, CPU order: pre before the core E
 // update, apply after Mur apply).  Elements sharing a field cell are grouped.
 struct RlcDev {

@@ -210,7 +210,9 @@ class CudaEngine:
                                              vp.ctypes.data_as(tp), nv, cp.ctypes.data_as(tp), nc))
 
     def configureLorentzADE(self, config):
-        """webgpu-engine.mjs:1358 — {orders: [{numCells, hasLorentz, directions: [...]}]}."""
+        """webgpu-engine.mjs:1358 — {orders: [{numCells, hasLorentz, directions: [...]}], apply}.
+        `apply` (default False) turns on the apply step the reference lacks
+        (efs_configure_ade_apply): the state is subtracted from E / H."""
         self._need_device()
         orders = config["orders"]
         oarr = (_lib.AdeOrder * max(1, len(orders)))()
@@ -235,6 +237,8 @@ class CudaEngine:
             oarr[i].num_directions = len(dirs)
             oarr[i].directions = darr
         self._ck(self._lib.efs_configure_ade(self._h, len(orders), oarr))
+        # opt-in apply step (no reference counterpart): subtract the state from the fields
+        self._ck(self._lib.efs_configure_ade_apply(self._h, 1 if config.get("apply") else 0))
 
     configureLorentz = configureLorentzADE   # name used by WebGPUFDTD / CPUFDTDEngine
 

@@ -335,6 +335,115 @@ def operator_dense(mesh, dT, eps_r=None, kappa=None, pec_edges=None, lumped_g=No
     return vv, vi, ii, iv
 
 
+# ---------------------------------------------------------------------------
+# Dispersive media: one Drude or Lorentz pole per E edge, as the inputs of
+# the engine's ADE extension (configureLorentzADE, src/webgpu-engine.mjs:1358)
+# with its apply step on.
+# ---------------------------------------------------------------------------
+# The reference has no generator for these inputs (no embind getter exists),
+# so they are derived here from the equivalent circuit: a dispersive E edge
+# carries, beside its capacitor C and conductance G, a branch current J
+# through an inductor L and resistor R (Drude: L = 1/(omega_p^2 C0),
+# R = gamma L) or through L, R and a capacitor C_L in series (Lorentz:
+# L = 1/(d_eps omega_0^2 C0), R = delta L, C_L = d_eps C0), C0 = eps0 A/l the
+# edge's vacuum capacitance.  The engine's state s is the branch current
+# scaled to volts (the term the apply step subtracts from V after the core
+# update V <- vv V + vi curl I); its update s <- v_int s + v_ext (V - lor),
+# lor <- lor + v_Lor s (src/webgpu-fdtd.mjs:405-454) runs before the core
+# update on the current V.
+#
+# "explicit": J at half steps, the branch equation centred on V^n (second
+# order; the coupling is explicit, stable while (omega_p dT)^2 / eps_r stays
+# well below 4): v_int = (1 - R dT/2L)/(1 + R dT/2L),
+# v_ext = vi dT / (L (1 + R dT/2L)), Lorentz v_Lor = dT / (C_L vi); the core
+# coefficients are unchanged.
+# "implicit": for stiff poles (a good conductor at microwave steps,
+# omega_p dT >> 1) the branch current is advanced with V^{n+1} (backward
+# Euler in the branch, L-stable), which folds into the core coefficients:
+# with a = 1/(1 + R dT/L), b = dT/(L + R dT):  vv' = vv/(1 + b vi),
+# vi' = vi/(1 + b vi), v_int = a, v_ext = a b vi/(1 + b vi).  (With the
+# trapezoidal loss of the core update, 1/vi = C/dT + G/2 and vv/vi =
+# C/dT - G/2.)
+
+
+def _edge_c0(vv, vi, dT, eps_r):
+    """Vacuum capacitance C0 = C/eps_r of E edges from their core coefficients
+    (vv = (1-g)/(1+g), vi = (dT/C)/(1+g), g = dT G / 2C), and the mask of
+    edges that have an update (vi > 0; metal edges and edges outside the
+    domain get no dispersive coupling: C0 is set to 1 there and their
+    coefficients are zeroed by the callers)."""
+    vv = np.asarray(vv, np.float64)
+    vi = np.asarray(vi, np.float64)
+    live = vi > 0
+    g = (1.0 - vv) / (1.0 + vv)
+    c0 = np.ones(vv.shape)
+    c0[live] = dT / (vi[live] * (1.0 + g[live])) / eps_r
+    return c0, live
+
+
+def ade_drude(vv, vi, dT, omega_p, gamma, eps_r=1.0, scheme="auto"):
+    """ADE inputs of a single-pole Drude medium on E edges with core
+    coefficients vv, vi (arrays, float64): dict(vv, vi, v_int, v_ext, scheme).
+    scheme "auto" picks "explicit" while (omega_p dT)^2 / eps_r < 1, else
+    "implicit" (see above)."""
+    vv = np.asarray(vv, np.float64)
+    vi = np.asarray(vi, np.float64)
+    c0, live = _edge_c0(vv, vi, dT, eps_r)
+    L = 1.0 / (omega_p * omega_p * c0)
+    if scheme == "auto":
+        scheme = "explicit" if (omega_p * dT) ** 2 / eps_r < 1.0 else "implicit"
+    if scheme == "explicit":
+        h = 1.0 + gamma * dT / 2.0
+        return dict(vv=vv, vi=vi, v_int=np.where(live, (1.0 - gamma * dT / 2.0) / h, 0.0),
+                    v_ext=np.where(live, vi * dT / (L * h), 0.0), scheme=scheme)
+    a = 1.0 / (1.0 + gamma * dT)
+    b = dT / (L * (1.0 + gamma * dT))
+    q = 1.0 + b * vi
+    return dict(vv=np.where(live, vv / q, vv), vi=np.where(live, vi / q, vi), v_int=np.where(live, a, 0.0),
+                v_ext=np.where(live, a * b * vi / q, 0.0), scheme="implicit")
+
+
+def ade_lorentz(vv, vi, dT, d_eps, omega_0, delta, eps_r=1.0):
+    """ADE inputs of a single-pole Lorentz medium (explicit scheme, see
+    above): dict(vv, vi, v_int, v_ext, v_lor, scheme)."""
+    vv = np.asarray(vv, np.float64)
+    vi = np.asarray(vi, np.float64)
+    c0, live = _edge_c0(vv, vi, dT, eps_r)
+    L = 1.0 / (d_eps * omega_0 * omega_0 * c0)
+    CL = d_eps * c0
+    h = 1.0 + delta * dT / 2.0
+    v_lor = np.zeros(vv.shape)
+    v_lor[live] = dT / (CL[live] * vi[live])
+    return dict(vv=vv, vi=vi, v_int=np.where(live, (1.0 - delta * dT / 2.0) / h, 0.0),
+                v_ext=np.where(live, vi * dT / (L * h), 0.0), v_lor=v_lor, scheme="explicit")
+
+
+def drude_eps(f, omega_p, gamma, eps_inf=1.0):
+    """Relative permittivity of a Drude pole at frequency f (e^{j omega t})."""
+    w = 2 * math.pi * np.asarray(f, np.float64)
+    return eps_inf - omega_p ** 2 / (w * (w - 1j * gamma))
+
+
+def lorentz_eps(f, d_eps, omega_0, delta, eps_inf=1.0):
+    """Relative permittivity of a Lorentz pole at frequency f (e^{j omega t})."""
+    w = 2 * math.pi * np.asarray(f, np.float64)
+    return eps_inf + d_eps * omega_0 ** 2 / (omega_0 ** 2 - w * w + 1j * w * delta)
+
+
+def slab_rt(f, eps, d):
+    """Normal-incidence reflection and transmission of a slab of relative
+    permittivity eps(f) and thickness d in vacuum (e^{j omega t}; T
+    referred to the slab's two faces)."""
+    k0 = 2 * math.pi * np.asarray(f, np.float64) / C0
+    n = np.sqrt(np.asarray(eps, np.complex128))
+    n = np.where(n.imag > 0, -n, n)                 # decaying branch for e^{j omega t}
+    r = (1 - n) / (1 + n)
+    p = np.exp(-1j * k0 * n * d)
+    R = r * (1 - p * p) / (1 - r * r * p * p)
+    T = (1 - r * r) * p / (1 - r * r * p * p)
+    return R, T
+
+
 def flat(a):
     """(3, Nx, Ny, Nz) -> NIJK float32 vector."""
     return np.ascontiguousarray(a, dtype=np.float32).reshape(-1)

@@ -262,19 +262,25 @@ def _dispersive_chunk(args):
 
 
 def dispersive(grid=(800, 800, 400), delta=0.25e-3, seed=5, pml=8, cover=0.3, nfreq=5, steps=40000, tfsf_inset=20,
-               nf2ff_inset=10, angle_deg=30.0, chunk=16, workers=None):
+               nf2ff_inset=10, angle_deg=30.0, chunk=16, workers=None, apply=True):
     """Plain dispersive solve: a uniform grid (800 x 800 x 400 lines, 0.25 mm),
     `pml`-cell UPML on all faces, seeded spheres (numpy default_rng(seed),
-    radius 5-40 cells, smaller on small grids) covering `cover` of the cells,
-    each single-pole Drude (omega_p = 1.4e16 rad/s, gamma = 3e13 1/s) or
-    Lorentz (delta_eps = 2, omega_0 = 2 pi 15 GHz, delta = 2 pi 1 GHz), a TFSF
+    radius 5-40 cells, smaller on small grids) inside the TFSF box covering
+    `cover` of all cells (on small grids at most half of that box), each
+    single-pole Drude (omega_p = 1.4e16 rad/s, gamma = 3e13 1/s) or Lorentz
+    (delta_eps = 2, omega_0 = 2 pi 15 GHz, delta = 2 pi 1 GHz), a TFSF
     Gaussian plane wave (10 GHz +- 5 GHz) at `angle_deg` from +z in the xz
-    plane, NF2FF with `nfreq` frequencies.  The spheres carry ADE state only:
-    the reference updates the auxiliary voltages every step and never applies
-    them to E or H (webgpu-fdtd.mjs:405-454, :1129-1172), so the ADE
-    coefficients here are a plain single-pole discretisation whose values do
-    not reach the fields.  Only the voltage side has coefficients; the
-    current side is all zero."""
+    plane, NF2FF with `nfreq` frequencies.
+
+    The media are the ADE extension's inputs from opgen.ade_drude /
+    opgen.ade_lorentz with the apply step on (`apply`): the Lorentz pole
+    with the explicit scheme, the stiff Drude pole (omega_p dT ~ 6.7e3) with
+    the implicit one, whose Drude cells get their own core coefficients (a
+    material-table row).  With apply=False the job is the reference's
+    state-only form: the same ADE inputs, vacuum core coefficients, and the
+    dispersion never reaches the fields (webgpu-fdtd.mjs:405-454,
+    :1129-1172).  Only the voltage side has coefficients; the current side
+    is all zero."""
     Nx, Ny, Nz = grid
     N = Nx * Ny * Nz
     mesh = opgen.Mesh(*[opgen.uniform_lines(n, delta) for n in grid])
@@ -286,17 +292,22 @@ def dispersive(grid=(800, 800, 400), delta=0.25e-3, seed=5, pml=8, cover=0.3, nf
     mat = np.empty(N, np.uint32)
     for x0, x1, m, tab in _parallel_map(_dispersive_chunk, items, workers):
         mat[x0 * Ny * Nz:x1 * Ny * Nz] = mt.add(tab)[m]
-    table = mt.table()
     regions = opgen.upml_apply(mesh, dT, _upml_boxes(grid, pml), [opgen.pml_sigma(mesh, a, pml, pml) for a in range(3)],
                                build=True)
-    # spheres: label 1 = Drude, 2 = Lorentz; a later sphere never relabels a cell
+    # spheres: label 1 = Drude, 2 = Lorentz; a later sphere never relabels a
+    # cell.  Spheres lie inside the TFSF box with a 2-cell margin (the total
+    # field region), away from the UPML and the injection surface.
     rng = np.random.default_rng(seed)
     label = np.zeros(grid, np.uint8)
     covered = 0
-    rmax = min(40, min(grid) // 2 - 1)
-    while covered < cover * N:
+    lo_c = tfsf_inset + 2
+    room = min(n - 1 - tfsf_inset - 2 - lo_c for n in grid)
+    rmax = max(1, min(40, room // 2 - 1))
+    box = int(np.prod([n - 1 - tfsf_inset - 2 - lo_c + 1 for n in grid]))
+    target = min(cover * N, 0.5 * box)        # small grids: at most half of the box the spheres may fill
+    while covered < target:
         r = int(rng.integers(min(5, rmax), rmax + 1))
-        c = [int(rng.integers(r, n - r)) for n in grid]
+        c = [int(rng.integers(lo_c + r, n - 1 - tfsf_inset - 2 - r + 1)) for n in grid]
         kind = 1 if rng.random() < 0.5 else 2
         sl = tuple(slice(c[a] - r, c[a] + r + 1) for a in range(3))
         ax = np.arange(-r, r + 1) ** 2
@@ -305,28 +316,35 @@ def dispersive(grid=(800, 800, 400), delta=0.25e-3, seed=5, pml=8, cover=0.3, nf
         new = ball & (sub == 0)
         sub[new] = kind
         covered += int(new.sum())
-    eps0 = opgen.EPS0
-    wp, gam = 1.4e16, 3e13
-    d_int = (1 - gam * dT / 2) / (1 + gam * dT / 2)
-    d_ext = eps0 * wp * wp * dT * delta / (1 + gam * dT / 2)
-    w0, dl, de = 2 * math.pi * 15e9, 2 * math.pi * 1e9, 2.0
-    l_int = (1 - dl * dT) / (1 + dl * dT)
-    l_ext = eps0 * de * w0 * w0 * dT * delta / (1 + dl * dT)
-    l_lor = w0 * w0 * dT * dT
-    orders = []
     flat = label.reshape(-1)
-    for kind, has_lor in ((1, False), (2, True)):
-        cells = np.flatnonzero(flat == kind).astype(np.uint32)
-        n = len(cells)
+    cells = [np.flatnonzero(flat == kind).astype(np.uint32) for kind in (1, 2)]
+    del label, flat
+    # ADE inputs from the sphere cells' core coefficients (one material row:
+    # uniform vacuum inside the TFSF box)
+    table = mt.table()
+    probe = cells[0][0] if len(cells[0]) else cells[1][0]
+    row = table[mat[probe]].astype(np.float64)
+    drude = [opgen.ade_drude(row[n:n + 1], row[3 + n:4 + n], dT, 1.4e16, 3e13) for n in range(3)]
+    lorentz = [opgen.ade_lorentz(row[n:n + 1], row[3 + n:4 + n], dT, 2.0, 2 * math.pi * 15e9, 2 * math.pi * 1e9)
+               for n in range(3)]
+    if apply and drude[0]["scheme"] == "implicit" and len(cells[0]):
+        drow = row.copy()
+        for n in range(3):
+            drow[n], drow[3 + n] = drude[n]["vv"][0], drude[n]["vi"][0]
+        did = np.uint32(mt.add(drow[None, :].astype(np.float32))[0])
+        mat[cells[0]] = did
+        table = mt.table()
+    orders = []
+    for kind, co, has_lor in ((1, drude, False), (2, lorentz, True)):
+        n = len(cells[kind - 1])
         dirs = []
         for d in range(3):
-            e = dict(dir=d, pos_idx=cells, v_int_ADE=np.full(n, d_int if kind == 1 else l_int, np.float32),
-                     v_ext_ADE=np.full(n, d_ext if kind == 1 else l_ext, np.float32))
+            e = dict(dir=d, pos_idx=cells[kind - 1], v_int_ADE=np.full(n, co[d]["v_int"][0], np.float32),
+                     v_ext_ADE=np.full(n, co[d]["v_ext"][0], np.float32))
             if has_lor:
-                e["v_Lor_ADE"] = np.full(n, l_lor, np.float32)
+                e["v_Lor_ADE"] = np.full(n, co[d]["v_lor"][0], np.float32)
             dirs.append(e)
         orders.append(dict(numCells=n, hasLorentz=has_lor, directions=dirs))
-    del label, flat
     f0, fc = 10e9, 5e9
     sig = opgen.gauss_signal(f0, fc, dT, steps).astype(np.float32)
     th = math.radians(angle_deg)
@@ -340,12 +358,13 @@ def dispersive(grid=(800, 800, 400), delta=0.25e-3, seed=5, pml=8, cover=0.3, nf
     pts, meta, primal, dual = opgen.nf2ff_box(mesh, [nf2ff_inset] * 3, [n - 1 - nf2ff_inset for n in grid])
     freqs = [f0 + fc * (k - (nfreq - 1) / 2) / max(1, nfreq - 1) for k in range(nfreq)]
     return dict(name="dispersive", grid=list(grid), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
-                coefficients=dict(mat=mat, table=table), pml=regions, ade=dict(orders=orders),
+                coefficients=dict(mat=mat, table=table), pml=regions, ade=dict(orders=orders, apply=bool(apply)),
                 tfsf=dict(signal=sig, period=0, voltagePoints=vp, currentPoints=cp),
                 nf2ff=dict(surfaceIndices=pts.ravel(), numPoints=len(pts), omegas=[2 * math.pi * f for f in freqs],
                            dT=dT, gridSize=list(grid), primalEdgeLens=primal, dualEdgeLens=dual, maxTS=steps,
                            windowType=0),
-                nf2ff_meta=meta, nf2ff_freqs=freqs, dispersive_cells=covered)
+                nf2ff_meta=meta, nf2ff_freqs=freqs, dispersive_cells=covered, dispersive_target=target,
+                sphere_box=(lo_c, [n - 1 - tfsf_inset - 2 for n in grid]))
 
 
 def _stub_filter_one(args):
@@ -600,3 +619,67 @@ def run_probe_job(engine, job):
     if job.get("include_t0"):
         v = np.concatenate([[0.0], v])
     return v
+
+
+def slab_1d(medium=None, delta=0.5e-3, nz=2400, z_src=50, z_r=400, slab=(800, 840), z_t=1200, steps=4700,
+            f0=8e9, fc=6e9):
+    """Plane wave through a dispersive slab, for checking the ADE apply step
+    against the analytic single-pole response.  A 4 x 4 x `nz` grid with
+    periodic x and y (configurePBC: fields stay uniform across the period)
+    and Mur on the z faces; an x-polarised soft source (Gaussian f0 +- fc) on
+    the plane z_src; the slab fills the E edges at nodes slab[0] .. slab[1]-1
+    (dual cells, thickness (slab[1]-slab[0]) * delta).  medium: None
+    (vacuum), ("drude", omega_p, gamma) or ("lorentz", d_eps, omega_0,
+    delta).  probe_idx: Ex field indices at z_r (before the slab) and z_t
+    (after it), sampled every step."""
+    grid = (4, 4, nz)
+    Nx, Ny, Nz = grid
+    mesh = opgen.Mesh(*[opgen.uniform_lines(n, delta) for n in grid])
+    dT = opgen.cfl_dt(mesh)
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, bc=(-1, -1, -1, -1, 0, 0))
+    job = dict(name="slab_1d", grid=list(grid), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh)
+    if medium is not None:
+        z1, z2 = slab
+        cells = np.array([x * Ny * Nz + y * Nz + z for x in range(Nx) for y in range(Ny) for z in range(z1, z2)],
+                         np.uint32)
+        xs, ys, zs = cells // (Ny * Nz), (cells // Nz) % Ny, cells % Nz
+        dirs, lor = [], medium[0] == "lorentz"
+        for n in range(3):
+            if lor:
+                c = opgen.ade_lorentz(vv[n][xs, ys, zs], vi[n][xs, ys, zs], dT, *medium[1:])
+            else:
+                c = opgen.ade_drude(vv[n][xs, ys, zs], vi[n][xs, ys, zs], dT, *medium[1:])
+            vv[n][xs, ys, zs] = c["vv"]
+            vi[n][xs, ys, zs] = c["vi"]
+            d = dict(dir=n, pos_idx=cells, v_int_ADE=c["v_int"].astype(np.float32),
+                     v_ext_ADE=c["v_ext"].astype(np.float32))
+            if lor:
+                d["v_Lor_ADE"] = c["v_lor"].astype(np.float32)
+            dirs.append(d)
+        job["ade"] = dict(orders=[dict(numCells=len(cells), hasLorentz=lor, directions=dirs)], apply=True)
+        job["ade_scheme"] = c["scheme"]
+    job["coefficients"] = dict(vv=opgen.flat(vv), vi=opgen.flat(vi), ii=opgen.flat(ii), iv=opgen.flat(iv))
+    sig = opgen.gauss_signal(f0, fc, dT, steps).astype(np.float32)
+    # the source covers the periodic cells (x, y < 3; the last line of each
+    # periodic axis is outside the period and stays quiet)
+    pos = [x * Ny * Nz + y * Nz + z_src for x in range(Nx - 1) for y in range(Ny - 1)]
+    job["excitation"] = dict(signal=sig, delay=[0] * len(pos), amp=[1.0] * len(pos), dir=[0] * len(pos), pos=pos,
+                             period=0)
+    job["mur"] = opgen.mur_dual(mesh, dT, [(2, "lo"), (2, "hi")])
+    job["pbc"] = dict(axes=[dict(axis=0, phase=0.0), dict(axis=1, phase=0.0)])
+    job["probe_idx"] = [1 * Ny * Nz + 1 * Nz + z_r, 1 * Ny * Nz + 1 * Nz + z_t]
+    job["slab"] = slab
+    job["z_r"], job["z_t"], job["delta"] = z_r, z_t, delta
+    return job
+
+
+def run_slab_1d(engine, job):
+    """Configure `job` (slab_1d) on `engine`, run it, return the Ex series at
+    the two probes (steps x 2)."""
+    configure(engine, job)
+    engine.configureProbeGatherBuffered(job["probe_idx"], maxSamples=job["maxTS"], sampleInterval=1)
+    engine.iterate(job["maxTS"])
+    r = engine.readProbeGatherBuffered()
+    g = np.asarray(r["data"], np.float64).reshape(r["numSamples"], r["stride"])
+    return g[:, 0::2]
+

@@ -138,6 +138,17 @@ typedef struct {
 
 efs_status efs_configure_ade(efs_engine* e, uint32_t count, const efs_ade_order* orders);
 
+/* Opt-in ADE apply step (on != 0), off by default and after every efs_init.
+ * The reference updates the ADE state and never applies it to the fields
+ * (src/webgpu-fdtd.mjs:405-454, step order :1129-1172), so dispersion never
+ * reaches E or H there.  With the step on, each entry's state is subtracted
+ * from its field, in configuration order: E entries after the
+ * apply-to-voltages phase (excitation, Mur apply, RLC apply), H entries after
+ * the post-current phase (TFSF, PBC) -- openEMS's Apply2Voltages /
+ * Apply2Current semantics.  No counterpart in the reference's API; the JS
+ * class maps configureLorentzADE({orders, apply: true}) to it. */
+efs_status efs_configure_ade_apply(efs_engine* e, int on);
+
 /* Lumped RLC element, same 48-byte packing as configureRLC (:1738-1756). */
 typedef struct {
     uint32_t field_idx;

@@ -11,7 +11,13 @@
 //       - updateCurrents        :113-155  (forward curl, loops to N-1)
 //       - applyExcitation       :161-185  (C++ past-end semantics: signal[0])
 //       - UPML pre/post         :239-358
-//       - Lorentz/Drude ADE     :381-454
+//       - Lorentz/Drude ADE     :381-454 (state update), plus an opt-in
+//         apply step the reference lacks: after the apply-to-voltages block
+//         (and after the post-current block for H) every ADE entry's state
+//         is subtracted from its field, entry by entry in configuration
+//         order (openEMS Engine_Ext_Dispersive Apply2Voltages /
+//         Apply2Current semantics); off by default, which is the
+//         reference's state-only behaviour
 //       - TFSF                  :681-733
 //       - lumped RLC            :750-863
 //       - Mur ABC 3-phase       :941-1023
@@ -115,6 +121,7 @@ struct Engine : EngineBase {
     };
     struct ADEOrder { uint32_t numCells; bool lorentz; std::vector<ADEDir> dirs; };
     std::vector<ADEOrder> ade;
+    bool ade_apply = false;   // subtract the ADE state from the fields after the core update
 
     // RLC
     struct RLCElem { uint32_t field_idx, direction, type_flag; float i2v, ilv, vvd, vv2, vj1, vj2, ib0, b1, b2; };
@@ -292,6 +299,21 @@ struct Engine : EngineBase {
                     } else {
                         st[i] = S(C(ki[i]) * C(st[i]) + C(ke[i]) * C(V));
                     }
+                }
+            }
+    }
+
+    // Opt-in apply step (no counterpart in the reference engine): F -= state,
+    // every (order, direction, cell) entry in configuration order.
+    template <bool VOLT>
+    void applyADE() {
+        for (auto& o : ade)
+            for (auto& d : o.dirs) {
+                std::vector<S>& F = VOLT ? volt : curr;
+                const std::vector<S>& st = VOLT ? d.vade : d.cade;
+                for (uint32_t i = 0; i < o.numCells; ++i) {
+                    S& f = F[(size_t)d.dir * N + d.pos[i]];
+                    f = S(C(f) - C(st[i]));
                 }
             }
     }
@@ -528,6 +550,7 @@ struct Engine : EngineBase {
         applyExcitation();
         murApply();
         applyRLC();
+        if (ade_apply) applyADE<true>();
         // CURRENT
         pmlPass<false, true>();
         updateADE<false>();
@@ -535,6 +558,7 @@ struct Engine : EngineBase {
         pmlPass<false, false>();
         applyTFSF<false>();
         pbcCopy<false>();
+        if (ade_apply) applyADE<false>();
         // accumulation passes that follow a step (webgpu-engine.mjs:2483-2499)
         nf2ffAccumulate(numTS + 1);
         gather();
@@ -719,6 +743,14 @@ void or_add_ade(void* h, uint32_t order, uint32_t numCells, int lorentz, uint32_
     });
 }
 
+// Opt-in ADE apply step (see applyADE)
+void or_set_ade_apply(void* h, int on) {
+    dispatch(static_cast<EngineBase*>(h), [&](auto* e) {
+        e->ade_apply = on != 0;
+        return 0;
+    });
+}
+
 // RLC elements as 12 columns: field_idx, direction, type_flag (u32) then
 // i2v ilv vvd vv2 vj1 vj2 ib0 b1 b2 (f32)
 void or_configure_rlc(void* h, uint32_t n, const uint32_t* field_idx, const uint32_t* direction, const uint32_t* type_flag,
@@ -825,6 +857,8 @@ int or_phase(void* h, const char* name) {
         else if (s == "postCurrentUpdatePML") e->template pmlPass<false, false>();
         else if (s == "updateVoltADE") e->template updateADE<true>();
         else if (s == "updateCurrADE") e->template updateADE<false>();
+        else if (s == "applyVoltADE") e->template applyADE<true>();
+        else if (s == "applyCurrADE") e->template applyADE<false>();
         else if (s == "applyTFSFVoltage") e->template applyTFSF<true>();
         else if (s == "applyTFSFCurrent") e->template applyTFSF<false>();
         else if (s == "preVoltageRLC") e->preVoltageRLC();

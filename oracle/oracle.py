@@ -47,6 +47,7 @@ def load():
             "or_configure_mur": (None, [vp, f32p, u32p, u32p, u32]),
             "or_configure_tfsf": (None, [vp, f32p, u32, u32, u32p, u32p, f32p, f32p, u32, u32p, u32p, f32p, f32p, u32]),
             "or_add_ade": (None, [vp, u32, u32, C.c_int, u32, u32p, f32p, f32p, f32p, f32p, f32p, f32p]),
+            "or_set_ade_apply": (None, [vp, C.c_int]),
             "or_configure_rlc": (None, [vp, u32, u32p, u32p, u32p, f32p]),
             "or_configure_steady_state": (None, [vp, u32p, u32, u32, C.c_float]),
             "or_set_steady_state": (None, [vp, C.c_int, u32]),
@@ -240,6 +241,7 @@ class OracleEngine:
                        ("v_int_ADE", "v_ext_ADE", "v_Lor_ADE", "i_int_ADE", "i_ext_ADE", "i_Lor_ADE")]
                 self._lib.or_add_ade(self._h, oi, int(o["numCells"]), 1 if o.get("hasLorentz") else 0, int(d["dir"]),
                                      _p(pos, C.c_uint32), *[_p(a, C.c_float) for a in arr])
+        self._lib.or_set_ade_apply(self._h, 1 if cfg.get("apply") else 0)
 
     configureLorentzADE = configureLorentz
 

@@ -3,8 +3,9 @@ oracle, for the dispersive and the large plain workloads at reduced sizes
 (the FP64 oracle finishes them in seconds).
 
 Dispersive: workloads.dispersive at 48 x 40 x 32 (UPML on all faces,
-Drude/Lorentz spheres, TFSF at 30 degrees, NF2FF with 5 frequencies), 600
-steps.  Plain: workloads.large_plain(64) (boxes, Mur, UPML on z, TFSF, NF2FF
+Drude/Lorentz spheres with the ADE apply step on, so the dispersion reaches
+the fields; TFSF at 30 degrees, NF2FF with 5 frequencies), 1200 steps (the
+pulse through the spheres).  Plain: workloads.large_plain(64) (boxes, Mur, UPML on z, TFSF, NF2FF
 with 3 frequencies), 800 steps.  Compared: E and H (relative L2), the energy
 at every 100-step checkpoint (relative to its peak), the ADE state (relative
 L2) and Dmax at every NF2FF frequency, from the engine's own far-field
@@ -67,8 +68,9 @@ def _statement(cls, job, steps, name):
 
 def test_dispersive_against_f64(cuda_engine_cls):
     from efs_b200 import workloads
-    job = workloads.dispersive(grid=(48, 40, 32), pml=4, chunk=8, steps=600, tfsf_inset=8, nf2ff_inset=6, workers=1)
-    out = _statement(cuda_engine_cls, job, 600, "dispersive 48x40x32")
+    job = workloads.dispersive(grid=(48, 40, 32), pml=4, chunk=8, steps=1200, tfsf_inset=8, nf2ff_inset=6, workers=1)
+    assert job["ade"]["apply"]
+    out = _statement(cuda_engine_cls, job, 1200, "dispersive 48x40x32 (ADE applied)")
     assert out["volt_relL2"] <= 1e-4 and out["curr_relL2"] <= 1e-4, out
     assert out["ade_volt_relL2"] <= 1e-4 and out["ade_volt_lor_relL2"] <= 1e-4, out
     assert out["energy_max_rel"] <= 1e-3 and out["Dmax_max_rel"] <= 1e-3, out

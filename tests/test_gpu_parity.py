@@ -286,7 +286,11 @@ def test_tfsf_on_tile_seams_bitexact(cuda_engine_cls):
         assert_bitexact(g.debugRead("pml_curr_flux", k), o.read("pml_curr_flux", k), "cflux %d" % k)
 
 
-def test_ade_in_and_out_of_pml_bitexact(cuda_engine_cls):
+@pytest.mark.parametrize("apply", [False, True])
+def test_ade_in_and_out_of_pml_bitexact(cuda_engine_cls, apply):
+    """Two orders on the same cells (with the apply step: entries grouped per
+    field location, applied in configuration order), both sides, some cells
+    inside a UPML slab."""
     N = (12, 10, 16)
     g, o = both(cuda_engine_cls, N, rand_coeffs(N, 18))
     regs = [pml_region((0, 0, 0), (12, 10, 4), 19)]
@@ -303,11 +307,50 @@ def test_ade_in_and_out_of_pml_bitexact(cuda_engine_cls):
         orders.append(dict(numCells=len(cells), hasLorentz=lor, directions=dirs))
     for e in (g, o):
         e.configurePML(regs)
-        e.configureLorentzADE({"orders": orders})
+        e.configureLorentzADE({"orders": orders, "apply": apply})
     seed_fields(g, o, N, 21)
     g.iterate(12)
     o.iterate(12)
-    compare_fields(g, o, "ade")
+    compare_fields(g, o, "ade apply=%s" % apply)
+    for name in ("ade_volt", "ade_volt_lor", "ade_curr", "ade_curr_lor"):
+        ref = np.concatenate([o.read(name, oi, d) for oi in range(2) for d in range(3)])
+        assert_bitexact(g.debugRead(name), ref, name)
+
+
+def test_ade_apply_runs_bitexact(cuda_engine_cls):
+    """Apply step with one entry per field location (entries stored as runs):
+    rows of ADE cells crossing a UPML slab, a TFSF point and an excitation on
+    ADE cells (their H neighbours are deferred twice over), Drude and Lorentz
+    orders on disjoint cells, both sides."""
+    N = (14, 11, 23)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 40))
+    regs = [pml_region((0, 0, 0), (14, 11, 4), 41)]
+    r = np.random.default_rng(42)
+    rows = [idx(0, x, y, 0, *N) for x in range(2, 12, 3) for y in range(1, 10, 2)]
+    cells = np.unique(np.concatenate([np.arange(c, c + 20) for c in rows]))   # z rows 0..19: runs
+    half = len(cells) // 2
+    orders = []
+    for lor, cl in ((False, cells[:half]), (True, cells[half:])):
+        k = len(cl)
+        dirs = [dict(dir=d, pos_idx=cl, v_int_ADE=0.5 + 0.4 * r.random(k), v_ext_ADE=0.05 * r.random(k),
+                     v_Lor_ADE=0.02 * r.random(k), i_int_ADE=0.5 + 0.4 * r.random(k), i_ext_ADE=0.05 * r.random(k),
+                     i_Lor_ADE=0.02 * r.random(k)) for d in range(3)]
+        orders.append(dict(numCells=k, hasLorentz=lor, directions=dirs))
+    c0 = int(cells[3])
+    sig = np.sin(np.arange(30) * 0.5).astype(np.float32)
+    tf = dict(signal=sig, period=0, voltagePoints=[dict(field_idx=c0, delay_int=1, delay_frac=0.25, amp=0.7)],
+              currentPoints=[dict(field_idx=int(N[0] * N[1] * N[2] + cells[7]), delay_int=0, delay_frac=0.5, amp=0.3)])
+    exc = dict(signal=sig, delay=[2], amp=[0.8], dir=[2], pos=[int(cells[10])], period=0)
+    for e in (g, o):
+        e.configurePML(regs)
+        e.configureLorentzADE({"orders": orders, "apply": True})
+        e.configureTFSF(tf)
+        e.configureExcitation(exc)
+    seed_fields(g, o, N, 43)
+    for n in (1, 9, 30):
+        g.iterate(n)
+        o.iterate(n)
+        compare_fields(g, o, "ade apply runs +%d" % n)
     for name in ("ade_volt", "ade_volt_lor", "ade_curr", "ade_curr_lor"):
         ref = np.concatenate([o.read(name, oi, d) for oi in range(2) for d in range(3)])
         assert_bitexact(g.debugRead(name), ref, name)
@@ -532,13 +575,16 @@ def test_openems_cavity_fixture_on_gpu(cuda_engine_cls):
     assert err < 1e-4, err
 
 
-def test_dispersive_small_bitexact(cuda_engine_cls):
+@pytest.mark.parametrize("apply", [True, False])
+def test_dispersive_small_bitexact(cuda_engine_cls, apply):
     """The dispersive workload at a small size: UPML on all faces, Drude and
     Lorentz ADE on the voltage side (the current side has all-zero
     coefficients and its kernel is skipped), TFSF at 30 degrees, NF2FF with 5
-    frequencies."""
+    frequencies; with the apply step (the default) and in the reference's
+    state-only form."""
     from efs_b200 import workloads
-    job = workloads.dispersive(grid=(48, 40, 32), pml=4, chunk=8, steps=200, tfsf_inset=8, nf2ff_inset=6, workers=1)
+    job = workloads.dispersive(grid=(48, 40, 32), pml=4, chunk=8, steps=200, tfsf_inset=8, nf2ff_inset=6, workers=1,
+                               apply=apply)
     g = cuda_engine_cls()
     assert g.initGPU()
     o = OracleEngine(mode="f32")

@@ -1,8 +1,9 @@
 """The dispersive job generator (workloads.dispersive) on a small grid, on the
-CPU: sphere coverage, the two media and their single-pole coefficients, the
-oblique TFSF and NF2FF inputs, determinism per seed, and an oracle run in
-which the voltage-side ADE state evolves while the all-zero current side
-stays exactly +0 (the case the CUDA engine skips)."""
+CPU: sphere coverage and placement, the two media and their single-pole
+coefficients (opgen.ade_drude / ade_lorentz, apply step on), the oblique TFSF
+and NF2FF inputs, determinism per seed, and an oracle run in which the
+voltage-side ADE state evolves while the all-zero current side stays exactly
++0 (the case the CUDA engine skips)."""
 import math
 
 import numpy as np
@@ -20,25 +21,41 @@ def small(seed=5):
 def test_coverage_media_and_coefficients():
     job = small()
     N = GRID[0] * GRID[1] * GRID[2]
-    assert 0.30 <= job["dispersive_cells"] / N < 0.40          # spheres stop once 30% is covered
+    target = job["dispersive_target"]
+    assert 0 < target <= 0.3 * N
+    assert target <= job["dispersive_cells"] < target + 4 * 4 * 4 * 8   # spheres stop once the target is covered
     orders = job["ade"]["orders"]
+    assert job["ade"]["apply"] is True
     assert [o["hasLorentz"] for o in orders] == [False, True]
     assert sum(o["numCells"] for o in orders) == job["dispersive_cells"]
-    cells = [set(np.asarray(o["directions"][0]["pos_idx"]).tolist()) for o in orders]
-    assert not (cells[0] & cells[1])                          # a cell belongs to one medium
-    dT, delta = job["dT"], 0.25e-3
-    wp, gam = 1.4e16, 3e13
-    d_int = (1 - gam * dT / 2) / (1 + gam * dT / 2)
-    d_ext = opgen.EPS0 * wp * wp * dT * delta / (1 + gam * dT / 2)
-    w0, dl, de = 2 * math.pi * 15e9, 2 * math.pi * 1e9, 2.0
-    for o, (ki, ke) in zip(orders, ((d_int, d_ext), ((1 - dl * dT) / (1 + dl * dT),
-                                                     opgen.EPS0 * de * w0 * w0 * dT * delta / (1 + dl * dT)))):
-        assert len(o["directions"]) == 3
-        for d in o["directions"]:
-            assert np.all(d["v_int_ADE"] == np.float32(ki)) and np.all(d["v_ext_ADE"] == np.float32(ke))
-            assert "i_int_ADE" not in d                       # the current side has no coefficients
-    lor = orders[1]["directions"][0]["v_Lor_ADE"]
-    assert np.all(lor == np.float32(w0 * w0 * dT * dT))
+    cells = [np.asarray(o["directions"][0]["pos_idx"]) for o in orders]
+    assert not (set(cells[0].tolist()) & set(cells[1].tolist()))      # a cell belongs to one medium
+    # spheres inside the TFSF box with a 2-cell margin
+    lo, hi = job["sphere_box"]
+    for c in cells:
+        xyz = np.stack([c // (GRID[1] * GRID[2]), (c // GRID[2]) % GRID[1], c % GRID[2]], 1)
+        assert xyz.min() >= lo and np.all(xyz <= np.asarray(hi))
+    # coefficients: the generator's Drude (implicit) and Lorentz (explicit) poles on the vacuum row
+    dT = job["dT"]
+    table, mat = job["coefficients"]["table"], job["coefficients"]["mat"]
+    vac = np.asarray(table[mat[cells[1][0]]], np.float64)                # Lorentz cells keep the vacuum row
+    drow = np.asarray(table[mat[cells[0][0]]], np.float64)
+    assert np.all(mat[cells[0]] == mat[cells[0][0]]) and np.all(mat[cells[1]] == mat[cells[1][0]])
+    for n in range(3):
+        dr = opgen.ade_drude(vac[n:n + 1], vac[3 + n:4 + n], dT, 1.4e16, 3e13)
+        lr = opgen.ade_lorentz(vac[n:n + 1], vac[3 + n:4 + n], dT, 2.0, 2 * math.pi * 15e9, 2 * math.pi * 1e9)
+        assert dr["scheme"] == "implicit" and lr["scheme"] == "explicit"
+        assert drow[n] == np.float32(dr["vv"][0]) and drow[3 + n] == np.float32(dr["vi"][0])
+        d0, d1 = orders[0]["directions"][n], orders[1]["directions"][n]
+        assert np.all(d0["v_int_ADE"] == np.float32(dr["v_int"][0])) and np.all(d0["v_ext_ADE"] == np.float32(dr["v_ext"][0]))
+        assert np.all(d1["v_int_ADE"] == np.float32(lr["v_int"][0])) and np.all(d1["v_ext_ADE"] == np.float32(lr["v_ext"][0]))
+        assert np.all(d1["v_Lor_ADE"] == np.float32(lr["v_lor"][0]))
+        assert "i_int_ADE" not in d0 and "i_int_ADE" not in d1           # the current side has no coefficients
+    # the state-only form keeps the vacuum row on the Drude cells
+    off = workloads.dispersive(grid=GRID, pml=4, chunk=8, steps=200, tfsf_inset=8, nf2ff_inset=6, workers=1, apply=False)
+    assert off["ade"]["apply"] is False
+    t2, m2 = off["coefficients"]["table"], off["coefficients"]["mat"]
+    assert np.array_equal(t2[m2[cells[0][0]]], t2[m2[cells[1][0]]])
 
 
 def test_tfsf_nf2ff_and_determinism():
