@@ -72,6 +72,7 @@ SIGNATURES = {
     "efs_configure_nf2ff": (C.c_int, [vp, u32p, u32, f64p, u32, C.c_double, f32p, u32, u32]),
     "efs_read_nf2ff": (C.c_int, [vp, f32p, f32p, szt]),
     "efs_far_field": (C.c_int, [vp, u32, f32p, f32p, u32, f32p, u32, f64p, C.c_double, C.c_double, f32p]),
+    "efs_far_field_time": (C.c_int, [vp, f32p]),
     "efs_energy": (C.c_int, [vp, C.c_int, f64p]),
     "efs_flush_energy": (C.c_int, [vp, f64p]),
     "efs_energy_noalloc": (C.c_int, [vp, f64p]),

@@ -226,6 +226,7 @@ struct efs_engine {
     bool nf_on = false;
     DevBuf nf_pts, nf_el, nf_E, nf_H, nf_samp;
     Nf2ffDev nf{};
+    float ff_ms[2] = {0.f, 0.f};     // device time of the last far-field call: point records, angle sums
 
     // energy (lagged, double-buffered like computeEnergy :2974-3021)
     DevBuf en_partial, en_result;
@@ -1398,39 +1399,65 @@ efs_status efs_far_field(efs_engine* e, uint32_t fi, const float* meta, const fl
         e->need_init();
         if (!e->nf_on) fail(EFS_ERR_STATE, "NF2FF not configured");
         if (fi >= e->nf.nf) fail(EFS_ERR_INVALID, "frequency index out of range");
-        if (!meta || !theta || !phi || !out || nth == 0 || nph == 0) fail(EFS_ERR_INVALID, "far-field arguments invalid");
+        if (!meta || !theta || !phi || !out || !center || nth == 0 || nph == 0) fail(EFS_ERR_INVALID, "far-field arguments invalid");
         const uint32_t np = e->nf.np;
-        const uint32_t A = nth * nph;
-        DevBuf dm, dth, dph, dpart, dout;
+        const uint64_t A64 = (uint64_t)nth * nph;
+        if (A64 >= (1ull << 31)) fail(EFS_ERR_RANGE, "too many far-field angles");
+        const uint32_t A = (uint32_t)A64;
+        // points grouped by the normal axis of their face (counting sort, stable)
+        std::vector<uint32_t> perm(np);
+        FarFieldDev d;
+        memset(&d, 0, sizeof(d));
+        {
+            uint32_t cnt[4] = {0, 0, 0, 0};
+            for (uint32_t p = 0; p < np; ++p) {
+                const float nd = meta[8 * (size_t)p + 3];
+                if (!(nd == 0.f || nd == 1.f || nd == 2.f)) fail(EFS_ERR_INVALID, "pointMeta normal direction must be 0, 1 or 2");
+                ++cnt[(int)nd + 1];
+            }
+            for (int n = 0; n < 3; ++n) cnt[n + 1] += cnt[n];
+            for (int n = 0; n < 4; ++n) d.seg[n] = cnt[n];
+            for (uint32_t p = 0; p < np; ++p) perm[cnt[(int)meta[8 * (size_t)p + 3]]++] = p;
+        }
+        DevBuf dm, dperm, drec, dth, dph, dout;
         e->upload(dm, meta, 8 * (size_t)np);
+        e->upload(dperm, perm);
         e->upload(dth, theta, nth);
         e->upload(dph, phi, nph);
-        // split points so that angle-blocks x chunks covers the SMs a few times
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
-        uint32_t ablocks = blocks(A, FF_THREADS);
-        uint32_t chunks = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)(4 * sms) / std::max<uint32_t>(ablocks, 1), blocks(np, FF_TILE)));
-        uint32_t chunk = (uint32_t)(((size_t)np + chunks - 1) / chunks);
-        chunk = ((chunk + FF_TILE - 1) / FF_TILE) * FF_TILE;
-        chunks = std::max<uint32_t>(1, blocks(np, chunk));
-        e->alloc(dpart, (size_t)chunks * A * 8 * 4, false);
+        e->alloc(drec, (size_t)np * sizeof(FfRecord), false);
         e->alloc(dout, (size_t)A * 5 * 4, false);
         const double C0 = 299792458.0;
         const double k = 2 * M_PI * freq / C0;
-        FarFieldDev d;
-        d.np = np; d.nth = nth; d.nph = nph; d.chunk = chunk;
-        d.k = (float)k; d.cx = (float)center[0]; d.cy = (float)center[1]; d.cz = (float)center[2];
-        d.accE = e->nf_E.as<float>() + (size_t)fi * np * 6;
-        d.accH = e->nf_H.as<float>() + (size_t)fi * np * 6;
-        d.meta = dm.as<float>(); d.theta = dth.as<float>(); d.phi = dph.as<float>(); d.partial = dpart.as<float>();
-        k_far_field<<<dim3(ablocks, chunks), FF_THREADS, 0, e->stream>>>(d);
         const double fmag = k / (4 * M_PI * radius), fph = -k * radius;   // (:2880-2884)
-        k_far_field_final<<<blocks(A, 256), 256, 0, e->stream>>>(dpart.as<float>(), A, chunks, fmag * (-std::sin(fph)),
-                                                                   fmag * std::cos(fph), dout.as<float>());
+        d.np = np; d.nth = nth; d.nph = nph;
+        d.rec = drec.as<FfRecord>();
+        d.theta = dth.as<float>(); d.phi = dph.as<float>();
+        d.fre = fmag * (-std::sin(fph)); d.fim = fmag * std::cos(fph);
+        d.out = dout.as<float>();
+        cudaEvent_t ev[3];
+        for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+        ck(cudaEventRecord(ev[0], e->stream), "record");
+        k_ff_prep<<<blocks(np, 256), 256, 0, e->stream>>>(dm.as<float>(), e->nf_E.as<float>() + (size_t)fi * np * 6,
+                                                          e->nf_H.as<float>() + (size_t)fi * np * 6, dperm.as<uint32_t>(), np,
+                                                          (float)(k / (2 * M_PI)), (float)center[0], (float)center[1],
+                                                          (float)center[2], drec.as<FfRecord>());
+        ck(cudaEventRecord(ev[1], e->stream), "record");
+        k_ff_angles<<<blocks(A, FF_ANG), FF_THREADS, 0, e->stream>>>(d);
+        ck(cudaEventRecord(ev[2], e->stream), "record");
         ck(cudaGetLastError(), "far field");
         ck(cudaMemcpyAsync(out, dout.p, (size_t)A * 5 * 4, cudaMemcpyDeviceToHost, e->stream), "read far field");
         e->sync("sync");
+        cudaEventElapsedTime(&e->ff_ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&e->ff_ms[1], ev[1], ev[2]);
+        for (auto& x : ev) cudaEventDestroy(x);
     });
+}
+
+efs_status efs_far_field_time(const efs_engine* e, float* ms) {
+    if (!e || !ms) return EFS_ERR_INVALID;
+    ms[0] = e->ff_ms[0];
+    ms[1] = e->ff_ms[1];
+    return EFS_OK;
 }
 
 static void energy_launch(efs_engine* e, int slot) {

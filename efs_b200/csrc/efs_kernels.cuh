@@ -662,92 +662,123 @@ __global__ void __launch_bounds__(256) k_energy_ranges(const float* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// NF2FF far field (src/webgpu-engine.mjs:830-985).  Thread = one (theta,phi)
-// angle; a block stages a tile of surface points in shared memory (surface
-// currents Js = n x H, Ms = -n x E precomputed per point) and every thread
-// sweeps the tile.  blockIdx.y splits the points so the grid fills the SMs;
-// k_far_field_final sums the chunks in f64 and forms E_theta, E_phi, P_rad.
+// NF2FF far field (src/webgpu-engine.mjs:830-985): per angle (theta, phi),
+//   N = sum_p area_p J_p e^{j k r^.r_p},  L = sum_p area_p M_p e^{j k r^.r_p}
+// with the surface currents J = n x H, M = -n x E of each point's face, then
+// E_theta, E_phi and the radiated intensity from the theta/phi projections.
+//
+// k_ff_prep turns every point into a 48-byte record: its position times
+// k / 2 pi (the phase comes out in turns) and the two tangential components
+// of area*J and area*M (a face with normal axis n carries currents along
+// a = n+1 and b = n+2 only), with the points ordered by normal axis (the
+// host passes the permutation).  k_ff_angles: a block takes FF_ANG angles; a
+// warp holds FF_ANG/8 angles x FF_PL point lanes; the block stages tiles of
+// records in shared memory and each thread sums its angle over every
+// FF_PL-th point of the tile in f32 (only the two tangential accumulators of
+// the segment's normal axis are live), adding the tile's sum into f64
+// accumulators; the FF_PL point lanes of an angle are combined with warp
+// shuffles and one lane forms the result in f64.  The phase is reduced to
+// [-1/2, 1/2] turns before the hardware sine/cosine (error ~2^-21 there).
 // ---------------------------------------------------------------------------
 constexpr int FF_THREADS = 256;
-constexpr int FF_TILE = 256;
+constexpr int FF_PL = 4;                                  // point lanes per angle (a shuffle group)
+constexpr int FF_ANG = FF_THREADS / FF_PL;                // angles per block
+constexpr int FF_TILE = 512;                              // records per shared-memory tile
+struct FfRecord { float4 pos; float4 j; float4 m; };     // pos: x,y,z in turns (w unused); j, m: a_re a_im b_re b_im
 struct FarFieldDev {
-    uint32_t np, nth, nph, chunk;
-    float k, cx, cy, cz;
-    const float* accE; const float* accH; const float* meta;
+    uint32_t np, nth, nph;
+    uint32_t seg[4];                                      // records of normal axis n: [seg[n], seg[n+1])
+    const FfRecord* rec;
     const float* theta; const float* phi;
-    float* partial;          // [chunks][A][8]
+    double fre, fim;                                      // k/(4 pi r) e^{-j k r} factor (re, im)
+    float* out;                                           // 5 per angle
 };
-__global__ void __launch_bounds__(FF_THREADS) k_far_field(const FarFieldDev d) {
-    __shared__ float sp[FF_TILE][16];   // pos xyz, area, J re/im xyz, M re/im xyz
-    const uint32_t A = d.nth * d.nph;
-    const uint32_t a = blockIdx.x * FF_THREADS + threadIdx.x;
-    const bool live = a < A;
-    float sT = 0, cT = 0, sP = 0, cP = 0;
-    if (live) {
-        const float th = d.theta[a / d.nph], ph = d.phi[a % d.nph];
-        sincosf(th, &sT, &cT);
-        sincosf(ph, &sP, &cP);
-    }
-    const float cTcP = cT * cP, cTsP = cT * sP, sTcP = sT * cP, sTsP = sT * sP;
-    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const uint32_t p0 = blockIdx.y * d.chunk, p1 = min(p0 + d.chunk, d.np);
+// One record per point, in the order perm (points grouped by normal axis).
+__global__ void k_ff_prep(const float* __restrict__ meta, const float* __restrict__ accE, const float* __restrict__ accH,
+                          const uint32_t* __restrict__ perm, uint32_t np, float kx, float cx, float cy, float cz,
+                          FfRecord* __restrict__ rec) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const uint32_t p = perm[i];
+    const float* m = meta + 8 * (size_t)p;
+    const float* E = accE + 6 * (size_t)p;
+    const float* H = accH + 6 * (size_t)p;
+    const int nd = (int)m[3];
+    const int ca = (nd + 1) % 3, cb = (nd + 2) % 3;
+    const float s = m[4] * m[5];                          // normal sign x area
+    FfRecord r;
+    r.pos = make_float4((m[0] - cx) * kx, (m[1] - cy) * kx, (m[2] - cz) * kx, 0.f);
+    // J_a = -s H_b, J_b = s H_a; M_a = s E_b, M_b = -s E_a  (J = n x H, M = -n x E)
+    r.j = make_float4(-s * H[2 * cb], -s * H[2 * cb + 1], s * H[2 * ca], s * H[2 * ca + 1]);
+    r.m = make_float4(s * E[2 * cb], s * E[2 * cb + 1], -s * E[2 * ca], -s * E[2 * ca + 1]);
+    rec[i] = r;
+}
+// Records [p0, p1) of normal axis ND for this thread's angle (direction u).
+template <int ND>
+__device__ __forceinline__ void ff_segment(const FarFieldDev& d, FfRecord* tile, uint32_t p0, uint32_t p1, float ux, float uy,
+                                           float uz, int q, bool live, double acc[12]) {
+    constexpr int CA = (ND + 1) % 3, CB = (ND + 2) % 3;
     for (uint32_t t0 = p0; t0 < p1; t0 += FF_TILE) {
         const uint32_t nt = min((uint32_t)FF_TILE, p1 - t0);
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < nt; j += FF_THREADS) {
-            const uint32_t p = t0 + j;
-            const float* m = d.meta + 8 * (size_t)p;
-            const float* E = d.accE + 6 * (size_t)p;
-            const float* H = d.accH + 6 * (size_t)p;
-            const int nd = (int)m[3];
-            const float s = m[4];
-            float J[6] = {0, 0, 0, 0, 0, 0}, M[6] = {0, 0, 0, 0, 0, 0};   // [comp*2 + re/im]
-            for (int c = 0; c < 2; ++c) {
-                if (nd == 0) { J[2 + c] = -s * H[4 + c]; J[4 + c] = s * H[2 + c]; M[2 + c] = s * E[4 + c]; M[4 + c] = -s * E[2 + c]; }
-                else if (nd == 1) { J[0 + c] = s * H[4 + c]; J[4 + c] = -s * H[0 + c]; M[0 + c] = -s * E[4 + c]; M[4 + c] = s * E[0 + c]; }
-                else { J[0 + c] = -s * H[2 + c]; J[2 + c] = s * H[0 + c]; M[0 + c] = s * E[2 + c]; M[2 + c] = -s * E[0 + c]; }
-            }
-            sp[j][0] = m[0] - d.cx; sp[j][1] = m[1] - d.cy; sp[j][2] = m[2] - d.cz; sp[j][3] = m[5];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) { sp[j][4 + q] = J[q]; sp[j][10 + q] = M[q]; }
-        }
+        for (uint32_t j = threadIdx.x; j < nt; j += FF_THREADS) tile[j] = d.rec[t0 + j];
         __syncthreads();
-        if (live) {
-            for (uint32_t j = 0; j < nt; ++j) {
-                const float* q = sp[j];
-                const float rc = q[0] * sTcP + q[1] * sTsP + q[2] * cT;
-                float sn, cs;
-                sincosf(d.k * rc, &sn, &cs);
-                const float ar = q[3] * cs, ai = q[3] * sn;
-                const float Jtr = q[4] * cTcP + q[6] * cTsP - q[8] * sT, Jti = q[5] * cTcP + q[7] * cTsP - q[9] * sT;
-                const float Jpr = q[6] * cP - q[4] * sP, Jpi = q[7] * cP - q[5] * sP;
-                const float Mtr = q[10] * cTcP + q[12] * cTsP - q[14] * sT, Mti = q[11] * cTcP + q[13] * cTsP - q[15] * sT;
-                const float Mpr = q[12] * cP - q[10] * sP, Mpi = q[13] * cP - q[11] * sP;
-                acc[0] += ar * Jtr - ai * Jti; acc[1] += ar * Jti + ai * Jtr;
-                acc[2] += ar * Jpr - ai * Jpi; acc[3] += ar * Jpi + ai * Jpr;
-                acc[4] += ar * Mtr - ai * Mti; acc[5] += ar * Mti + ai * Mtr;
-                acc[6] += ar * Mpr - ai * Mpi; acc[7] += ar * Mpi + ai * Mpr;
-            }
+        if (!live) continue;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // N_a, N_b, L_a, L_b (re, im)
+        for (uint32_t j = q; j < nt; j += FF_PL) {
+            const FfRecord& r = tile[j];
+            float ph = r.pos.x * ux;
+            ph = fmaf(r.pos.y, uy, ph);
+            ph = fmaf(r.pos.z, uz, ph);
+            ph -= rintf(ph);                                   // turns in [-1/2, 1/2]
+            float sn, cs;
+            __sincosf(6.2831853071795864f * ph, &sn, &cs);
+            s[0] = fmaf(r.j.x, cs, fmaf(-r.j.y, sn, s[0])); s[1] = fmaf(r.j.y, cs, fmaf(r.j.x, sn, s[1]));
+            s[2] = fmaf(r.j.z, cs, fmaf(-r.j.w, sn, s[2])); s[3] = fmaf(r.j.w, cs, fmaf(r.j.z, sn, s[3]));
+            s[4] = fmaf(r.m.x, cs, fmaf(-r.m.y, sn, s[4])); s[5] = fmaf(r.m.y, cs, fmaf(r.m.x, sn, s[5]));
+            s[6] = fmaf(r.m.z, cs, fmaf(-r.m.w, sn, s[6])); s[7] = fmaf(r.m.w, cs, fmaf(r.m.z, sn, s[7]));
         }
-    }
-    if (live) {
-        float* o = d.partial + ((size_t)blockIdx.y * A + a) * 8;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) o[q] = acc[q];
+        acc[2 * CA] += s[0]; acc[2 * CA + 1] += s[1];
+        acc[2 * CB] += s[2]; acc[2 * CB + 1] += s[3];
+        acc[6 + 2 * CA] += s[4]; acc[6 + 2 * CA + 1] += s[5];
+        acc[6 + 2 * CB] += s[6]; acc[6 + 2 * CB + 1] += s[7];
     }
 }
-__global__ void k_far_field_final(const float* partial, uint32_t A, uint32_t chunks, double fre, double fim, float* out) {
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A) return;
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t c = 0; c < chunks; ++c)
-        for (int q = 0; q < 8; ++q) s[q] += (double)partial[((size_t)c * A + a) * 8 + q];
+__global__ void __launch_bounds__(FF_THREADS) k_ff_angles(const FarFieldDev d) {
+    __shared__ FfRecord tile[FF_TILE];
+    const int lane = threadIdx.x & 31, q = lane % FF_PL;
+    const uint32_t A = d.nth * d.nph;
+    const uint32_t a = blockIdx.x * FF_ANG + threadIdx.x / FF_PL;
+    const bool live = a < A;
+    float sT = 0.f, cT = 1.f, sP = 0.f, cP = 1.f;
+    if (live) {
+        sincosf(d.theta[a / d.nph], &sT, &cT);
+        sincosf(d.phi[a % d.nph], &sP, &cP);
+    }
+    const float ux = sT * cP, uy = sT * sP, uz = cT;
+    double acc[12];                                      // N_x, N_y, N_z, L_x, L_y, L_z (re, im)
+#pragma unroll
+    for (int i = 0; i < 12; ++i) acc[i] = 0.0;
+    ff_segment<0>(d, tile, d.seg[0], d.seg[1], ux, uy, uz, q, live, acc);
+    ff_segment<1>(d, tile, d.seg[1], d.seg[2], ux, uy, uz, q, live, acc);
+    ff_segment<2>(d, tile, d.seg[2], d.seg[3], ux, uy, uz, q, live, acc);
+    // the FF_PL point lanes of this angle are adjacent lanes of one warp
+#pragma unroll
+    for (int i = 0; i < 12; ++i)
+#pragma unroll
+        for (int o = 1; o < FF_PL; o <<= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+    if (!live || q != 0) return;
+    const double cTcP = (double)cT * cP, cTsP = (double)cT * sP;
+    auto proj_t = [&](int b, int c) { return acc[b + c] * cTcP + acc[b + 2 + c] * cTsP - acc[b + 4 + c] * (double)sT; };
+    auto proj_p = [&](int b, int c) { return acc[b + 2 + c] * (double)cP - acc[b + c] * (double)sP; };
+    const double Ntr = proj_t(0, 0), Nti = proj_t(0, 1), Npr = proj_p(0, 0), Npi = proj_p(0, 1);
+    const double Ltr = proj_t(6, 0), Lti = proj_t(6, 1), Lpr = proj_p(6, 0), Lpi = proj_p(6, 1);
     const double Z0 = 376.73031346177066;
-    const double ar = s[6] + Z0 * s[0], ai = s[7] + Z0 * s[1];
-    const double Etr = -(fre * ar - fim * ai), Eti = -(fre * ai + fim * ar);
-    const double br = s[4] - Z0 * s[2], bi = s[5] - Z0 * s[3];
-    const double Epr = fre * br - fim * bi, Epi = fre * bi + fim * br;
-    float* o = out + 5 * (size_t)a;
+    const double ar = Lpr + Z0 * Ntr, ai = Lpi + Z0 * Nti;
+    const double Etr = -(d.fre * ar - d.fim * ai), Eti = -(d.fre * ai + d.fim * ar);
+    const double br = Ltr - Z0 * Npr, bi = Lti - Z0 * Npi;
+    const double Epr = d.fre * br - d.fim * bi, Epi = d.fre * bi + d.fim * br;
+    float* o = d.out + 5 * (size_t)a;
     o[0] = (float)((Etr * Etr + Eti * Eti + Epr * Epr + Epi * Epi) / (2 * Z0));
     o[1] = (float)Etr; o[2] = (float)Eti; o[3] = (float)Epr; o[4] = (float)Epi;
 }

@@ -371,6 +371,12 @@ class CudaEngine:
             return {"accumE": e.reshape(nf, npts * 6), "accumH": h.reshape(nf, npts * 6)}
         return {"accumE": e[:npts * 6].copy(), "accumH": h[:npts * 6].copy()}
 
+    def farFieldTime(self):
+        """Device ms of the last far-field call: [point records, angle sums]."""
+        ms = np.zeros(2, np.float32)
+        self._ck(self._lib.efs_far_field_time(self._h, _p(ms, C.c_float)))
+        return [float(ms[0]), float(ms[1])]
+
     def computeNF2FFfarField(self, config):
         """webgpu-engine.mjs:2871 — {pointMeta, theta, phi, center, frequency, radius, numPoints[, freqIndex]}
         -> 5 floats per angle (P_rad, Et_re, Et_im, Ep_re, Ep_im)."""

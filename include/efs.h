@@ -224,6 +224,11 @@ efs_status efs_far_field(efs_engine* e, uint32_t freq_index, const float* point_
                          const float* theta, uint32_t n_theta, const float* phi, uint32_t n_phi,
                          const double center[3], double frequency, double radius, float* out);
 
+/* Diagnostics: device time (ms) of the last efs_far_field call's two kernels:
+ * ms[0] the per-point records, ms[1] the angle sums.  No counterpart in the
+ * reference. */
+efs_status efs_far_field_time(const efs_engine* e, float* ms);
+
 /* --- energy ------------------------------------------------------------ */
 
 /* computeEnergy (:2974-3021): sum over the (Nx-1)(Ny-1)(Nz-1) interior
