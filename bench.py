@@ -45,6 +45,16 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-timesteps", type=int, default=2, help="timesteps per reference-arm step")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-sweep measurement")
+    p.add_argument("--no-patch", action="store_true", help="skip the patch-antenna solve")
+    p.add_argument("--cpu-timesteps", type=int, default=40, help="timesteps of the CPU-baseline sample")
+    p.add_argument("--no-far-field", action="store_true", help="skip the 181 x 361 far-field measurement")
+    p.add_argument("--no-dispersive", action="store_true", help="skip the 800 x 800 x 400 dispersive solve")
+    p.add_argument("--dispersive-timesteps", type=int, default=200, help="timed timesteps of the dispersive solve")
+    p.add_argument("--no-served", action="store_true", help="skip the served request stream")
+    p.add_argument("--served-arrivals-s", type=float, default=10.0, help="seconds of 20 req/s arrivals (saturated legs)")
+    p.add_argument("--served-horizon-s", type=float, default=40.0, help="serving time of the saturated legs")
+    p.add_argument("--served-capacity-rate", type=float, default=0.5, help="req/s of the capacity-matched leg")
+    p.add_argument("--served-capacity-s", type=float, default=40.0, help="seconds of capacity-matched arrivals")
     p.add_argument("--batch-count", type=int, default=64, help="instances of the batched sweep")
     return p.parse_args()
 
@@ -198,7 +208,7 @@ def batched_sweep(args, local):
     cells = sum(j["grid"][0] * j["grid"][1] * j["grid"][2] for j in jobs)
     b = CudaBatch(engines)
     tuned = b.autotune(steps=8)                  # real timesteps, identical results under every shape
-    T = 192                                      # timesteps per member in each timed leg (3 graphs of 64)
+    T = 1024                                     # timesteps per member in each timed leg (16 graphs of 64)
     b.iterate(T)
     b.sync()
     t0 = time.perf_counter()
@@ -225,6 +235,188 @@ def batched_sweep(args, local):
             "batched_solves_per_s_15000_steps": round(v_b * 1e6 / (cells / len(jobs)) / 15000, 3),
             "sequential_solves_per_s_15000_steps": round(v_s * 1e6 / (cells / len(jobs)) / 15000, 3),
             "autotuned": tuned, "timing": "wall clock around device-synchronised runs of %d timesteps" % T}
+
+
+def patch_solve(local):
+    """The plain single solve of the reference's published benchmark: the
+    86 x 87 x 71 patch antenna (graded mesh, UPML 8, 50-ohm port, probes every
+    step), 30 000 timesteps through the orchestrator's loop (iterate(100) +
+    lagged energy, sim-engine.mjs:648-681).  Device time by CUDA events on the
+    engine stream; the published figures are for the same grid and step count
+    (README.md:137-140 of the reference; the WebGPU figure recomputed from its
+    6.2 s)."""
+    import torch
+    from efs_b200 import workloads
+    from efs_b200.engine import CudaEngine
+    job = workloads.patch_antenna()
+    N = job["grid"][0] * job["grid"][1] * job["grid"][2]
+    g = CudaEngine(device=local)
+    g.initGPU()
+    workloads.configure(g, job)
+    stream = torch.cuda.ExternalStream(g.stream)
+    for _ in range(5):
+        g.iterate(100)
+        g.computeEnergy()
+    g.sync()
+    T = job["maxTS"]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(T // 100):
+        g.iterate(100)
+        g.computeEnergy()
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - t0
+    ms = ev0.elapsed_time(ev1)
+    g.destroy()
+    return {"workload": "patch antenna 86x87x71 graded mesh, UPML 8, 50-ohm port, probes every step",
+            "cells": N, "timesteps": T, "mcells_s": round(N * T / (ms / 1e3) / 1e6, 1), "seconds": round(ms / 1e3, 3),
+            "wall_s": round(wall, 3),
+            "published_30000_steps": {"openems_multithreaded_mcells_s": 444, "openems_multithreaded_s": 36,
+                                      "webgpu_mcells_s": 2570, "webgpu_s": 6.2,
+                                      "note": "reference README.md:137-140 (their hardware, Mur boundaries)"}}
+
+
+FF_FLOPS_PER_PAIR = 40     # per (angle, point): 3 FMA phase + 2 phase reduction + 16 FMA (4 complex MACs)
+
+
+def fp32_peak_tflops(device):
+    """Nominal FP32 (non-tensor) peak: SMs x 128 lanes x 2 flops x max SM clock."""
+    import torch
+    props = torch.cuda.get_device_properties(device)
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(device), "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=20)
+        mhz = float(out.stdout.strip().splitlines()[0])
+    except Exception:
+        mhz = 1965.0
+    return props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def far_field_leg(eng, job, local):
+    """The NF2FF far field of the headline job at its configured size: a
+    181 x 361 theta/phi grid (1-degree steps) at each of the 3 frequencies,
+    on the accumulators of the timed run (computeNF2FFfarField through the
+    public API).  GFLOP/s counts FF_FLOPS_PER_PAIR per (angle, point) pair
+    over the angle kernel's device time; e2e is the call's wall time (point
+    metadata upload, both kernels, result readback)."""
+    theta = np.deg2rad(np.arange(181, dtype=np.float64)).astype(np.float32)
+    phi = np.deg2rad(np.arange(361, dtype=np.float64)).astype(np.float32)
+    A = theta.size * phi.size
+    npts = job["nf2ff"]["numPoints"]
+    per = []
+    for fi, fr in enumerate(job["nf2ff_freqs"]):
+        cfg = dict(pointMeta=job["nf2ff_meta"], theta=theta, phi=phi, center=[0.0, 0.0, 0.0], frequency=fr, radius=1.0,
+                   numPoints=npts, freqIndex=fi)
+        eng.computeNF2FFfarField(cfg)                  # warm-up
+        t0 = time.perf_counter()
+        out = eng.computeNF2FFfarField(cfg)
+        wall = time.perf_counter() - t0
+        prep_ms, ang_ms = eng.farFieldTime()
+        per.append({"freq_GHz": round(fr / 1e9, 3), "angles_ms": round(ang_ms, 3), "prep_ms": round(prep_ms, 3),
+                    "call_wall_ms": round(1e3 * wall, 2), "P_max": float(np.asarray(out).reshape(-1, 5)[:, 0].max())})
+    pairs = float(A) * npts
+    ang = sum(p["angles_ms"] for p in per) / len(per)
+    gflops = pairs * FF_FLOPS_PER_PAIR / (ang / 1e3) / 1e9
+    peak = fp32_peak_tflops(local)
+    return {"angles": A, "grid": "181 x 361 (1 degree)", "points": npts, "frequencies": len(per),
+            "pairs_per_frequency": int(pairs), "flops_per_pair": FF_FLOPS_PER_PAIR,
+            "gflops": round(gflops, 1), "fp32_peak_tflops_nominal": round(peak, 1),
+            "frac_of_nominal_fp32": round(gflops / 1e3 / peak, 4),
+            "e2e_ms_per_frequency": round(sum(p["call_wall_ms"] for p in per) / len(per), 2), "per_frequency": per}
+
+
+def dispersive_leg(args, local):
+    """The plain dispersive solve of the configuration list at its full size:
+    800 x 800 x 400 lines, 0.25 mm, UPML 8 on all faces, Drude (stiff) and
+    Lorentz spheres over 30% of the cells with the ADE apply step on, TFSF at
+    30 degrees, NF2FF with 5 frequencies (workloads.dispersive).  Timed with
+    CUDA events on the engine stream over `--dispersive-timesteps` timesteps
+    after 2 x 100 warm-up timesteps."""
+    import torch
+    from efs_b200 import workloads
+    from efs_b200.engine import CudaEngine
+    t0 = time.perf_counter()
+    job = workloads.dispersive()
+    t_gen = time.perf_counter() - t0
+    N = job["grid"][0] * job["grid"][1] * job["grid"][2]
+    g = CudaEngine(device=local)
+    g.initGPU()
+    t0 = time.perf_counter()
+    workloads.configure(g, dict(job, probes=[]))
+    g.iterate(1)
+    g.sync()
+    t_cfg = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(g.stream)
+    for _ in range(2):
+        g.iterate(100)
+        g.computeEnergy()
+    g.sync()
+    T = max(1, args.dispersive_timesteps // 100) * 100
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(T // 100):
+        g.iterate(100)
+        g.computeEnergy()
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    out = {"workload": "dispersive 800x800x400, UPML8 all faces, Drude/Lorentz spheres 30% (ADE applied), TFSF 30 deg, "
+                       "NF2FF F=5", "cells": N, "dispersive_cells": int(job["dispersive_cells"]), "timesteps": T,
+           "ms_per_timestep": round(ms / T, 4), "mcells_s": round(N * T / (ms / 1e3) / 1e6, 1),
+           "kernels_per_timestep": g.kernelsPerStep(), "device_gb": round(g.deviceBytes() / 1e9, 2),
+           "host_generate_s": round(t_gen, 1), "host_configure_s": round(t_cfg, 1)}
+    g.destroy()
+    return out
+
+
+def _served_template(a):
+    from efs_b200 import workloads
+    kind, side, steps = a
+    return workloads.served_template(kind, side, steps=steps)
+
+
+def served_leg(args, local):
+    """The served request stream of the configuration list (Poisson arrivals,
+    cubic-ish grids with sides log-uniform in [40, 300], 70% lumped-port/Mur
+    jobs and 30% TFSF+NF2FF jobs with 2 frequencies, 5000-25000 steps, 150 GB
+    HBM budget; serve.request_stream, numpy default_rng(4)), in shortened
+    windows (the configuration's run is 10 minutes):
+      saturated:  20 req/s for --served-arrivals-s, served for --served-horizon-s,
+                  with continuous batching (64 member slots) and as a plain
+                  one-slot queue (the plain engine's sequential solves) on the
+                  same stream; throughput = cell-steps/s of each, solves/s =
+                  completions / horizon;
+      capacity:   --served-capacity-rate req/s for --served-capacity-s, drained:
+                  p50/p95/p99 latency near the device's capacity.
+    Request inputs are prepared before the clock starts."""
+    from efs_b200 import serve, workloads
+    sat = serve.request_stream(20.0, args.served_arrivals_s)
+    cap = serve.request_stream(args.served_capacity_rate, args.served_capacity_s, seed=5)
+    keys = sorted({(k, sd) for _, k, sd, _ in sat + cap})
+    t0 = time.perf_counter()
+    made = workloads._parallel_map(_served_template, [(k, sd, 25000) for k, sd in keys], min(len(keys), 8))
+    templates = dict(zip(keys, made))
+    prep = time.perf_counter() - t0
+
+    def one(stream, members, horizon):
+        srv = serve.Server(hbm_budget=150e9, max_members=members, chunk=256, device=local)
+        serve.run_stream(stream, templates, srv, horizon=horizon)
+        wall = srv.now()
+        srv.close()
+        done = srv.finished
+        return {"arrivals": len(stream), "completed": len(done), "wall_s": round(wall, 2),
+                "solves_per_s": round(len(done) / wall, 4), "mcells_s": round(srv.cell_steps / wall / 1e6, 1),
+                "latency": serve.latency_stats(done), "member_slots": members}
+    batched = one(sat, 64, args.served_horizon_s)
+    plain = one(sat, 1, args.served_horizon_s)
+    capacity = one(cap, 64, None)
+    return {"window": "shortened: %.0f s of 20 req/s arrivals served for %.0f s; %.2f req/s for %.0f s drained" % (
+                args.served_arrivals_s, args.served_horizon_s, args.served_capacity_rate, args.served_capacity_s),
+            "template_prep_s": round(prep, 1), "saturated_continuous": batched, "saturated_plain_queue": plain,
+            "throughput_ratio_vs_plain": round(batched["mcells_s"] / max(plain["mcells_s"], 1e-9), 3),
+            "capacity_matched": capacity}
 
 
 def run_b200(args):
@@ -296,6 +488,9 @@ def run_b200(args):
     chunks = [64] * (BATCH // 64) + ([BATCH % 64] if BATCH % 64 else [])
     nf_passes = sum(math.ceil(m / 16) for m in chunks) if job.get("nf2ff") else 0
     launches = args.steps * (BATCH * eng.kernelsPerStep() + len(chunks) + nf_passes + 2)
+    far = None
+    if rank == 0 and world == 1 and not args.no_far_field and job.get("nf2ff"):
+        far = far_field_leg(eng, job, local)
     eng.destroy()
 
     # end to end through the public API from host buffers
@@ -325,12 +520,22 @@ def run_b200(args):
         del en
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, threads, dt = cpu_sample(job, "js", 2)
+        v, threads, dt = cpu_sample(job, "js", args.cpu_timesteps)
         cpu = {"value": round(v, 3), "unit": "MCells/s", "cores": threads, "kind": "port",
-               "sample": "2 timesteps of the same %d^3 job on the CPU oracle (CPUFDTDEngine arithmetic), %.1f s" % (args.n, dt)}
+               "sample": "%d timesteps of the same %d^3 job on the CPU oracle (CPUFDTDEngine arithmetic), %.1f s" % (
+                   args.cpu_timesteps, args.n, dt)}
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_sweep(args, local)
+    patch = None
+    if rank == 0 and world == 1 and not args.no_patch:
+        patch = patch_solve(local)
+    disp = None
+    if rank == 0 and world == 1 and not args.no_dispersive:
+        disp = dispersive_leg(args, local)
+    served = None
+    if rank == 0 and world == 1 and not args.no_served:
+        served = served_leg(args, local)
     if rank == 0:
         print(json.dumps({
             "metric": "MCells/s", "value": round(value, 3), "unit": "MCells/s", "n_gpus": world,
@@ -348,6 +553,10 @@ def run_b200(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "batched": batched,
+            "patch": patch,
+            "far_field": far,
+            "dispersive": disp,
+            "served": served,
         }))
     if world > 1:
         import torch.distributed as dist
