@@ -47,6 +47,38 @@ def openems_cavity():
                 probes=[probe], include_t0=True)
 
 
+def openems_cavity_modes(steps=20000):
+    """The native-openEMS cavity-resonator fixture (reference
+    tests/generate_fixtures.py:63-178): 26x11x32 lines over 5x2x6 cm, PEC
+    walls, Gaussian f0 = 5.5 GHz / fc = 4.5 GHz on the staircase from node
+    (17,7,21) to (18,8,22), voltage probe on the z edge at (6,5,6) every 3
+    steps, `steps` steps at the mesh's Courant step (what openEMS picked:
+    the fixture's 1.14266409e-11 s sample spacing is 3 dT)."""
+    def lin(a, b, n):
+        st = (b - a) / (n - 1)
+        return [float("%.10e" % (a + i * st)) for i in range(n)]   # as written to the XML
+    mesh = opgen.Mesh(lin(0, 5e-2, 26), lin(0, 2e-2, 11), lin(0, 6e-2, 32))
+    dT = opgen.cfl_dt(mesh)
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT)
+    sig = opgen.gauss_signal(5.5e9, 4.5e9, dT, steps)
+    Nx, Ny, Nz = mesh.shape
+    ex = (Nx * 2 // 3, Ny * 2 // 3, Nz * 2 // 3)
+    p1 = [mesh.lines[k][i] for k, i in enumerate(ex)]
+    p2 = [mesh.lines[k][i + 1] for k, i in enumerate(ex)]
+    amp, dirs, pos = [], [], []
+    for n, (x, y, z) in opgen.find_path(mesh, p1, p2):
+        amp.append(mesh.dl(n)[(x, y, z)[n]])
+        dirs.append(n)
+        pos.append(x * Ny * Nz + y * Nz + z)
+    pr = (Nx // 4, Ny // 2, Nz // 5)
+    probe = opgen.voltage_probe(mesh, list(pr), [pr[0], pr[1], pr[2] + 1], 1.0, 3)
+    return dict(name="openems_cavity_modes", grid=list(mesh.shape), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+                coefficients=dict(vv=opgen.flat(vv), vi=opgen.flat(vi), ii=opgen.flat(ii), iv=opgen.flat(iv)),
+                excitation=dict(signal=sig.astype(np.float32), delay=[0] * len(amp), amp=np.float32(amp), dir=dirs,
+                                pos=pos, period=0),
+                probes=[probe], include_t0=True)
+
+
 class _ChunkCells:
     """Per-cell eps_r of the cells with x index in [xs, xe), looked up by global x slice."""
 

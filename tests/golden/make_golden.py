@@ -7,6 +7,10 @@ The outputs are committed so the tests never read the reference tree.
                           probe voltage vp, 251 samples every 2 steps from t=0
   openems_cavity_t.npy    the matching sample times (s)
   constants.json          physical constants of the fixtures
+  openems_cavity_modes.npz  cavity/reference.json: the 26x11x32 PEC cavity's probe
+                          voltage (6667 samples every 3 steps from t=0), its analytic
+                          TE/TM mode frequencies and the reference's analysis
+                          tolerances (tests/test_wasm.mjs:140-246)
   coax_ports.npz          coax/reference.json: port voltage and current series
                           (time_s, values), the analytic Z0 and the tolerance band
                           the reference's port test applies (tests/test_api.mjs:585-620)
@@ -38,4 +42,13 @@ np.savez(os.path.join(OUT, "coax_ports.npz"),
          it_time=np.asarray(coax["probe_it1"]["time_s"], np.float64), it=np.asarray(coax["probe_it1"]["voltage"], np.float64),
          z0=np.float64(coax["Z0_analytical_ohm"]), tol_upper=np.float64(coax["tolerances"]["upper_error"]),
          tol_lower=np.float64(coax["tolerances"]["lower_error"]))
+cav = json.load(open(os.path.join(fx, "cavity", "reference.json")))
+modes = dict(cav["te_modes"], **cav["tm_modes"])
+names = sorted(modes)
+np.savez(os.path.join(OUT, "openems_cavity_modes.npz"),
+         time_s=np.asarray(cav["probe_data"]["time_s"], np.float64), voltage=np.asarray(cav["probe_data"]["voltage"], np.float64),
+         mode_names=np.asarray(names), mode_freqs=np.asarray([modes[k] for k in names], np.float64),
+         tolerances=np.asarray([cav["tolerances"][k] for k in ("te_freq_rel", "tm_freq_lower_rel", "te_min_amplitude",
+                                                               "tm_min_amplitude")], np.float64),
+         dims=np.asarray([cav["dimensions_m"][k] for k in ("a", "b", "d")], np.float64))
 print("wrote", OUT)

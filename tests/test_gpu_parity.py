@@ -575,6 +575,24 @@ def test_openems_cavity_fixture_on_gpu(cuda_engine_cls):
     assert err < 1e-4, err
 
 
+def test_openems_cavity_modes_fixture_on_gpu(cuda_engine_cls):
+    """Native-openEMS cavity-resonator fixture (tests/fixtures/cavity, 26x11x32
+    PEC box, 20000 steps, 6667 probe samples) reproduced by the CUDA engine:
+    relative L2 of the probe voltage < 1e-4, and bit for bit the oracle's f32
+    series."""
+    from efs_b200 import workloads
+    g_ = np.load(os.path.join(ROOT, "tests", "golden", "openems_cavity_modes.npz"))
+    job = workloads.openems_cavity_modes()
+    g = cuda_engine_cls()
+    assert g.initGPU()
+    v = workloads.run_probe_job(g, job)
+    err = np.linalg.norm(v - g_["voltage"]) / np.linalg.norm(g_["voltage"])
+    assert err < 1e-4, err
+    vo = workloads.run_probe_job(OracleEngine(job["grid"], job["coefficients"], mode="f32"), job)
+    assert_bitexact(v.astype(np.float32), vo.astype(np.float32), "cavity modes probe")
+    g.destroy()
+
+
 @pytest.mark.parametrize("apply", [True, False])
 def test_dispersive_small_bitexact(cuda_engine_cls, apply):
     """The dispersive workload at a small size: UPML on all faces, Drude and
