@@ -25,7 +25,7 @@ def solo(job, steps):
     if job.get("nf2ff"):
         acc = e.readNF2FFAccumulation(True)
         out["nf2ff"] = (acc["accumE"], acc["accumH"])
-    out["energy"] = e.computeEnergy(lagged=False)
+    out["energy"] = e.energyNoAlloc()          # the reduction the server's retirement uses
     e.destroy()
     return out
 
