@@ -85,6 +85,8 @@ SIGNATURES = {
     "efs_batch_autotune": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "efs_get_fields": (C.c_int, [vp, f32p, f32p]),
     "efs_set_fields": (C.c_int, [vp, f32p, f32p]),
+    "efs_get_planes": (C.c_int, [vp, u32, u32, vp, vp]),
+    "efs_set_planes": (C.c_int, [vp, u32, u32, vp, vp]),
     "efs_get_state": (C.c_int, [vp, vp, szt, C.POINTER(szt)]),
     "efs_set_state": (C.c_int, [vp, vp, szt]),
     "efs_device_bytes": (C.c_int, [vp, C.POINTER(szt)]),

@@ -1576,6 +1576,40 @@ efs_status efs_get_fields(efs_engine* e, float* v, float* c) {
     });
 }
 
+// x-planes [x, x + count) of E and H, packed as (3, count, Ny*Nz) floats
+// (unpadded rows) at volt / curr; host or device memory (cudaMemcpyDefault).
+static void plane_copies(efs_engine* e, uint32_t x, uint32_t count, float* v, float* c, bool out) {
+    if ((uint64_t)x + count > e->Nx) fail(EFS_ERR_INVALID, "plane range beyond the grid");
+    const size_t rows = (size_t)count * e->Ny;
+    for (int n = 0; n < 3; ++n) {
+        const size_t dev_off = (size_t)n * e->Nd + (size_t)x * e->Ny * e->Pz;
+        const size_t pk_off = (size_t)n * rows * e->Nz;
+        float* bufs[2] = {v, c};
+        float* fields[2] = {e->vcur(), e->ccur()};
+        for (int k = 0; k < 2; ++k) {
+            if (!bufs[k]) continue;
+            if (out)
+                ck(cudaMemcpy2DAsync(bufs[k] + pk_off, (size_t)e->Nz * 4, fields[k] + dev_off, (size_t)e->Pz * 4,
+                                     (size_t)e->Nz * 4, rows, cudaMemcpyDefault, e->stream), "plane copy out");
+            else
+                ck(cudaMemcpy2DAsync(fields[k] + dev_off, (size_t)e->Pz * 4, bufs[k] + pk_off, (size_t)e->Nz * 4,
+                                     (size_t)e->Nz * 4, rows, cudaMemcpyDefault, e->stream), "plane copy in");
+        }
+    }
+    e->sync("plane copy");
+}
+
+efs_status efs_get_planes(efs_engine* e, uint32_t x, uint32_t count, float* volt, float* curr) {
+    return guard(e, [&] { e->need_init(); plane_copies(e, x, count, volt, curr, true); });
+}
+
+efs_status efs_set_planes(efs_engine* e, uint32_t x, uint32_t count, const float* volt, const float* curr) {
+    return guard(e, [&] {
+        e->need_init();
+        plane_copies(e, x, count, const_cast<float*>(volt), const_cast<float*>(curr), false);
+    });
+}
+
 efs_status efs_set_fields(efs_engine* e, const float* v, const float* c) {
     return guard(e, [&] {
         e->need_init();

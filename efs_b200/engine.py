@@ -411,6 +411,34 @@ class CudaEngine:
         return v.value
 
     # --- state --------------------------------------------------------
+    def getPlanes(self, x, count, out=None):
+        """x-planes [x, x+count) of E and H as (3, count, Ny*Nz) float32 arrays
+        (efs_get_planes).  `out` may be a pair of torch CUDA tensors of that
+        shape: the planes are then copied device to device."""
+        Ny, Nz = self.numLines[1], self.numLines[2]
+        if out is not None:
+            self._ck(self._lib.efs_get_planes(self._h, int(x), int(count), C.c_void_p(out[0].data_ptr()),
+                                              C.c_void_p(out[1].data_ptr())))
+            return out
+        v = np.empty((3, count, Ny * Nz), np.float32)
+        c = np.empty((3, count, Ny * Nz), np.float32)
+        self._ck(self._lib.efs_get_planes(self._h, int(x), int(count), v.ctypes.data_as(C.c_void_p),
+                                          c.ctypes.data_as(C.c_void_p)))
+        return v, c
+
+    def setPlanes(self, x, volt, curr):
+        """Overwrite x-planes [x, x+count) of E and H (efs_set_planes); numpy
+        arrays or torch CUDA tensors of shape (3, count, Ny*Nz)."""
+        count = volt.shape[1]
+        if hasattr(volt, "data_ptr"):
+            self._ck(self._lib.efs_set_planes(self._h, int(x), int(count), C.c_void_p(volt.data_ptr()),
+                                              C.c_void_p(curr.data_ptr())))
+            return
+        v = np.ascontiguousarray(volt, np.float32)
+        c = np.ascontiguousarray(curr, np.float32)
+        self._ck(self._lib.efs_set_planes(self._h, int(x), int(count), v.ctypes.data_as(C.c_void_p),
+                                          c.ctypes.data_as(C.c_void_p)))
+
     def getFields(self):
         n = 3 * self.totalCells
         v = np.zeros(n, np.float32)

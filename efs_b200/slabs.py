@@ -203,3 +203,47 @@ def exchange_dist(slab, world, get_planes, set_planes, send_recv):
     got = send_recv(r - 1 if r > 0 else None, out, r + 1 if r + 1 < world else None, hi_ghost)
     if got is not None and hi_ghost:
         set_planes(r, slab["x1"] - slab["g0"], got[0], got[1])
+
+
+class LocalSlabs:
+    """Every slab of a job on engines driven by this process (one GPU each,
+    or several on one GPU): configure, step and exchange ghost planes with
+    the engines' getPlanes/setPlanes.  make_engine(rank) returns an
+    initialised engine (CudaEngine or the oracle)."""
+
+    def __init__(self, job, world, make_engine):
+        from . import workloads
+        self.job = job
+        self.parts = split(job, world)
+        self.engines = []
+        for s, sub in self.parts:
+            e = make_engine(s["rank"])
+            workloads.configure(e, sub)
+            self.engines.append(e)
+
+    def _get(self, r, x, cnt):
+        return self.engines[r].getPlanes(x, cnt)
+
+    def _set(self, r, x, v, c):
+        self.engines[r].setPlanes(x, v, c)
+
+    def iterate(self, n):
+        for _ in range(n):
+            for e in self.engines:
+                e.iterate(1)
+            exchange([s for s, _ in self.parts], self._get, self._set)
+
+    def owned_fields(self):
+        """E and H of the whole grid assembled from the owned planes, (3, Nx, Ny*Nz) each."""
+        Nx, Ny, Nz = self.job["grid"]
+        vs, cs = [], []
+        for (s, _), e in zip(self.parts, self.engines):
+            v, c = e.getPlanes(s["x0"] - s["g0"], s["x1"] - s["x0"])
+            vs.append(v)
+            cs.append(c)
+        return np.concatenate(vs, axis=1), np.concatenate(cs, axis=1)
+
+    def destroy(self):
+        for e in self.engines:
+            if hasattr(e, "destroy"):
+                e.destroy()

@@ -262,6 +262,15 @@ efs_status efs_energy_noalloc(efs_engine* e, double* out);
 efs_status efs_get_fields(efs_engine* e, float* volt, float* curr);
 efs_status efs_set_fields(efs_engine* e, const float* volt, const float* curr);
 
+/* x-planes [x, x + count) of E (volt) and H (curr), packed as 3 components x
+ * count planes x Ny*Nz floats in the reference's NIJK order; either pointer
+ * may be NULL; host or device memory (the copy kind is inferred).  The ghost
+ * exchange of an x-slab decomposition (efs_b200/slabs.py) moves these planes
+ * between the engines of neighbouring slabs.  No counterpart in the
+ * reference. */
+efs_status efs_get_planes(efs_engine* e, uint32_t x, uint32_t count, float* volt, float* curr);
+efs_status efs_set_planes(efs_engine* e, uint32_t x, uint32_t count, const float* volt, const float* curr);
+
 /* Full resident state (fields, UPML flux, Mur, ADE, RLC, steady state, PBC,
  * probe ring, NF2FF accumulators, numTS) as one opaque blob.  buf == NULL
  * queries the size.  Restoring needs an engine with the same configuration.
