@@ -27,11 +27,14 @@ from .engine import CudaBatch, CudaEngine
 
 
 class Request:
-    __slots__ = ("rid", "job", "steps", "arrival", "admitted", "done", "engine", "remaining", "slices", "result", "cells")
+    __slots__ = ("rid", "job", "steps", "arrival", "admitted", "done", "engine", "remaining", "slices", "result", "cells",
+                 "saved", "evictions")
 
     def __init__(self, rid, job, steps, arrival):
         self.rid, self.job, self.steps, self.arrival = rid, job, int(steps), arrival
         self.admitted = self.done = None
+        self.saved = None                          # host copy of an evicted solve's state (efs_get_state)
+        self.evictions = 0
         self.engine = None
         self.remaining = int(steps)
         self.slices = None
@@ -60,9 +63,18 @@ def estimate_bytes(job):
 class Server:
     """Continuous-batching request loop.  hbm_budget: bytes the resident
     solves may hold; max_members: member slots of the batch; chunk: most
-    timesteps per scheduling round."""
+    timesteps per scheduling round.
 
-    def __init__(self, hbm_budget=150e9, max_members=64, chunk=256, device=0):
+    evict_ratio: when set, a waiting request that cannot be admitted (no slot
+    or no memory) and whose step count is at most 1/evict_ratio of the
+    largest remaining step count among the resident solves has that solve
+    evicted: its whole device state is copied to the host (efs_get_state),
+    its engine is freed, and it waits right behind the newcomer; it resumes
+    later on a fresh engine from that copy (efs_set_state), with the same
+    result as if it had never left.  A solve is evicted at most
+    `max_evictions` times."""
+
+    def __init__(self, hbm_budget=150e9, max_members=64, chunk=256, device=0, evict_ratio=None, max_evictions=1):
         self.budget = float(hbm_budget)
         self.max_members = int(max_members)
         self.chunk = int(chunk)
@@ -75,6 +87,9 @@ class Server:
         self.next_id = 0
         self.t0 = time.perf_counter()
         self.cell_steps = 0
+        self.evict_ratio = evict_ratio
+        self.max_evictions = int(max_evictions)
+        self.evicted = 0
 
     def now(self):
         return time.perf_counter() - self.t0
@@ -96,8 +111,12 @@ class Server:
             e = CudaEngine(device=self.device)
             e.initGPU()
             r.slices = workloads.configure(e, r.job)
+            if r.saved is not None:                             # an evicted solve resumes where it stopped
+                e.setState(r.saved)
+                r.saved = None
             r.engine = e
-            r.admitted = self.now()
+            if r.admitted is None:
+                r.admitted = self.now()
             self.used += e.deviceBytes()
             self.active.append(r)
             added = True
@@ -125,6 +144,33 @@ class Server:
         e.destroy()
         r.engine = None
         self.finished.append(r)
+
+    def _evict(self):
+        """Evict one resident solve for the head of the queue (see evict_ratio);
+        the batch must be idle.  Returns True when one was evicted."""
+        if not self.evict_ratio or not self.waiting or not self.active:
+            return False
+        head = self.waiting[0]
+        fits = len(self.active) < self.max_members and (self.used + estimate_bytes(head.job) <= self.budget)
+        if fits:
+            return False
+        cand = [r for r in self.active if r.evictions < self.max_evictions and r.remaining >= self.evict_ratio * head.steps]
+        if not cand:
+            return False
+        victim = max(cand, key=lambda r: r.remaining)
+        if self.batch is not None:
+            self.batch.destroy()
+            self.batch = None
+        e = victim.engine
+        victim.saved = e.getState()
+        self.used -= e.deviceBytes()
+        e.destroy()
+        victim.engine = None
+        victim.evictions += 1
+        self.evicted += 1
+        self.active = [r for r in self.active if r is not victim]
+        self.waiting.insert(1, victim)                          # right behind the newcomer
+        return True
 
     def _rebatch(self):
         if self.batch is not None:
@@ -163,7 +209,8 @@ class Server:
                 self.batch = None
             for r in done:
                 self._retire(r)
-        if done or admitted:
+        evicted = self._evict()
+        if done or admitted or evicted:
             self._rebatch()
         return True
 

@@ -81,3 +81,33 @@ def test_served_admission_respects_budget(cuda_engine_cls):
     finally:
         srv.close()
     assert [r.rid for r in srv.finished] == [0, 1, 2]
+
+
+def test_evicted_solve_resumes_bit_exact(cuda_engine_cls):
+    """With one member slot, a long solve is evicted (its state read to the host
+    and its engine freed) so a short request can run, then restored into a new
+    engine; both results equal the same requests run alone, bit for bit."""
+    from efs_b200 import workloads
+    from efs_b200.serve import Server
+    long_job = workloads.served_template("tfsf", 40, steps=600)
+    short_job = workloads.served_template("port", 40, steps=200)
+    srv = Server(hbm_budget=8e9, max_members=1, chunk=64, evict_ratio=2.0)
+    try:
+        lid = srv.submit(long_job, 500)
+        assert srv.round()
+        sid = srv.submit(short_job, 120)
+        while srv.round():
+            assert len(srv.active) <= 1
+    finally:
+        srv.close()
+    by = {r.rid: r for r in srv.finished}
+    assert srv.evicted == 1 and by[lid].evictions == 1
+    assert by[sid].done < by[lid].done
+    for rid, job, steps in ((lid, long_job, 500), (sid, short_job, 120)):
+        ref = solo(job, steps)
+        assert by[rid].result["energy"] == ref["energy"], rid
+        if "probes" in ref:
+            assert np.array_equal(by[rid].result["probes"], ref["probes"]), rid
+        if "nf2ff" in ref:
+            for a, b in zip(by[rid].result["nf2ff"], ref["nf2ff"]):
+                assert np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32)), rid

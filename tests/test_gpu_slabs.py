@@ -62,7 +62,9 @@ def test_planes_round_trip_device(cuda_engine_cls):
     g.getPlanes(4, 2, out=(dv, dc))
     ref_v = v0.reshape(3, N[0], -1)[:, 4:6]
     assert np.array_equal(dv.cpu().numpy(), ref_v)
-    g.setPlanes(1, dv * 2, dc * 2)
+    dv2, dc2 = dv * 2, dc * 2
+    torch.cuda.synchronize()                 # torch's stream finished the products before the engine's stream reads them
+    g.setPlanes(1, dv2, dc2)
     f = g.getFields()
     got = np.asarray(f["volt"]).reshape(3, N[0], -1)
     assert np.array_equal(got[:, 1:3], 2 * ref_v)

@@ -34,6 +34,12 @@ class FakeEngine:
     def destroy(self):
         self.destroyed = True
 
+    def getState(self):
+        return {"steps": self.steps}
+
+    def setState(self, blob):
+        self.steps = blob["steps"]
+
 
 class FakeBatch:
     log = []                                    # (members, steps, member bytes) per iterate
@@ -138,6 +144,49 @@ def test_retirement_energy_does_not_allocate(fake):
     s.submit(job(1100, 1000), 10, arrival=0.0)   # 1099^3 > 2^30 interior cells
     drain(s)
     assert sorted(FakeEngine.energy_log) == [(40, "noalloc"), (1100, "alloc")]
+
+
+def test_eviction_lets_a_short_request_pass(fake):
+    """With one member slot, a long solve is evicted (state to the host) when a
+    request of at most 1/4 of its remaining steps waits, resumes afterwards
+    from its saved state and still runs exactly its step count; without
+    eviction the short request waits for the long one."""
+    def run(evict):
+        s = serve.Server(hbm_budget=1e15, max_members=1, chunk=100, evict_ratio=4.0 if evict else None)
+        long_id = s.submit(job(40, 1000), 2000, arrival=0.0)
+        s.round()                                  # the long solve is resident
+        s.round()
+        short_id = s.submit(job(16, 1000), 150, arrival=0.0)
+        drain(s)
+        by = {r.rid: r for r in s.finished}
+        return s, by[long_id], by[short_id]
+    s, lng, sht = run(True)
+    assert s.evicted == 1 and lng.evictions == 1
+    assert lng.result["energy"] == 2000.0 and sht.result["energy"] == 150.0     # exact step counts
+    assert sht.done < lng.done                    # the short request finished first
+    s0, lng0, sht0 = run(False)
+    assert s0.evicted == 0 and sht0.done > lng0.done
+    assert s.used == 0
+
+
+def test_eviction_respects_the_limit_and_ratio(fake):
+    s = serve.Server(hbm_budget=1e15, max_members=1, chunk=100, evict_ratio=4.0, max_evictions=1)
+    a = s.submit(job(40, 1000), 1000, arrival=0.0)
+    s.round()
+    s.round()
+    s.submit(job(16, 1000), 500, arrival=0.0)     # not short enough: 500 > remaining / 4
+    s.submit(job(16, 1000), 50, arrival=0.0)
+    drain(s)
+    by = {r.rid: r for r in s.finished}
+    assert by[a].evictions == 0                   # the head of the queue decides, and it was too long
+    s = serve.Server(hbm_budget=1e15, max_members=1, chunk=100, evict_ratio=2.0, max_evictions=1)
+    a = s.submit(job(40, 1000), 3000, arrival=0.0)
+    s.round()
+    for _ in range(3):
+        s.submit(job(16, 1000), 100, arrival=0.0)
+    drain(s)
+    assert s.evicted == 1                         # at most once per solve
+    assert {r.rid: r for r in s.finished}[a].result["energy"] == 3000.0
 
 
 def test_request_stream_and_latency_stats():
