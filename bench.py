@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-far-field", action="store_true", help="skip the 181 x 361 far-field measurement")
     p.add_argument("--no-dispersive", action="store_true", help="skip the 800 x 800 x 400 dispersive solve")
     p.add_argument("--dispersive-timesteps", type=int, default=200, help="timed timesteps of the dispersive solve")
+    p.add_argument("--dispersive-batch", type=int, default=16,
+                   help="dispersive 200x200x100 solves of the batched dispersive form (0: skip)")
     p.add_argument("--no-served", action="store_true", help="skip the served request stream")
     p.add_argument("--served-arrivals-s", type=float, default=10.0, help="seconds of 20 req/s arrivals (saturated legs)")
     p.add_argument("--served-horizon-s", type=float, default=40.0, help="serving time of the saturated legs")
@@ -189,26 +191,22 @@ def run_reference(args):
     }))
 
 
-def batched_sweep(args, local):
-    """Batched form on the stub-filter sweep (64 microstrip filters, uneven
-    grids): every member advanced by one persistent fused launch per timestep
-    (efs_batch_*), against the same engines stepped one after another.  Both
-    legs run the same number of timesteps per member (graphs captured in an
-    identical warm-up leg) and are timed by the wall clock around
-    device-synchronised runs."""
+def batch_vs_sequential(jobs, T, local):
+    """Configure one engine per job, autotune the batch, then time T timesteps
+    per member batched and the same engines stepped one after another (each
+    leg after an identical untimed leg that captures its graphs).  Returns
+    (cells, batched MCells/s, sequential MCells/s, autotuned shape)."""
     from efs_b200 import workloads
     from efs_b200.engine import CudaBatch, CudaEngine
-    jobs = workloads.stub_filters(count=args.batch_count)
     engines = []
     for j in jobs:
         e = CudaEngine(device=local)
         e.initGPU()
-        workloads.configure(e, j)
+        workloads.configure(e, dict(j, probes=j.get("probes") or []))
         engines.append(e)
     cells = sum(j["grid"][0] * j["grid"][1] * j["grid"][2] for j in jobs)
     b = CudaBatch(engines)
     tuned = b.autotune(steps=8)                  # real timesteps, identical results under every shape
-    T = 1024                                     # timesteps per member in each timed leg (16 graphs of 64)
     b.iterate(T)
     b.sync()
     t0 = time.perf_counter()
@@ -227,8 +225,20 @@ def batched_sweep(args, local):
     b.destroy()
     for e in engines:
         e.destroy()
-    v_b = cells * T / t_batch / 1e6
-    v_s = cells * T / t_seq / 1e6
+    return cells, cells * T / t_batch / 1e6, cells * T / t_seq / 1e6, tuned
+
+
+def batched_sweep(args, local):
+    """Batched form on the stub-filter sweep (64 microstrip filters, uneven
+    grids): every member advanced by one persistent fused launch per timestep
+    (efs_batch_*), against the same engines stepped one after another.  Both
+    legs run the same number of timesteps per member (graphs captured in an
+    identical warm-up leg) and are timed by the wall clock around
+    device-synchronised runs."""
+    from efs_b200 import workloads
+    jobs = workloads.stub_filters(count=args.batch_count)
+    T = 1024                                     # timesteps per member in each timed leg (16 graphs of 64)
+    cells, v_b, v_s, tuned = batch_vs_sequential(jobs, T, local)
     return {"workload": "stub_filters x%d: per-axis U[60,180] lines, 0.2 mm, Mur, two 50-ohm ports" % len(jobs),
             "instances": len(jobs), "cells": cells, "timesteps_per_member": T,
             "batched_mcells_s": round(v_b, 1), "sequential_mcells_s": round(v_s, 1), "speedup": round(v_b / v_s, 3),
@@ -330,10 +340,12 @@ def far_field_leg(eng, job, local):
 def dispersive_leg(args, local):
     """The plain dispersive solve of the configuration list at its full size:
     800 x 800 x 400 lines, 0.25 mm, UPML 8 on all faces, Drude (stiff) and
-    Lorentz spheres over 30% of the cells with the ADE apply step on, TFSF at
-    30 degrees, NF2FF with 5 frequencies (workloads.dispersive).  Timed with
-    CUDA events on the engine stream over `--dispersive-timesteps` timesteps
-    after 2 x 100 warm-up timesteps."""
+    Lorentz spheres over 30% of the cells, TFSF at 30 degrees, NF2FF with 5
+    frequencies (workloads.dispersive).  Run twice on the same job: as the
+    reference's engine runs it (ADE state updated, not applied to the fields)
+    and with the ADE apply step on.  Each is timed with CUDA events on the
+    engine stream over `--dispersive-timesteps` timesteps after 2 x 100
+    warm-up timesteps."""
     import torch
     from efs_b200 import workloads
     from efs_b200.engine import CudaEngine
@@ -341,33 +353,48 @@ def dispersive_leg(args, local):
     job = workloads.dispersive()
     t_gen = time.perf_counter() - t0
     N = job["grid"][0] * job["grid"][1] * job["grid"][2]
-    g = CudaEngine(device=local)
-    g.initGPU()
-    t0 = time.perf_counter()
-    workloads.configure(g, dict(job, probes=[]))
-    g.iterate(1)
-    g.sync()
-    t_cfg = time.perf_counter() - t0
-    stream = torch.cuda.ExternalStream(g.stream)
-    for _ in range(2):
-        g.iterate(100)
-        g.computeEnergy()
-    g.sync()
-    T = max(1, args.dispersive_timesteps // 100) * 100
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(T // 100):
-        g.iterate(100)
-        g.computeEnergy()
-    ev1.record(stream)
-    ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    out = {"workload": "dispersive 800x800x400, UPML8 all faces, Drude/Lorentz spheres 30% (ADE applied), TFSF 30 deg, "
-                       "NF2FF F=5", "cells": N, "dispersive_cells": int(job["dispersive_cells"]), "timesteps": T,
-           "ms_per_timestep": round(ms / T, 4), "mcells_s": round(N * T / (ms / 1e3) / 1e6, 1),
-           "kernels_per_timestep": g.kernelsPerStep(), "device_gb": round(g.deviceBytes() / 1e9, 2),
-           "host_generate_s": round(t_gen, 1), "host_configure_s": round(t_cfg, 1)}
-    g.destroy()
+
+    def run(apply):
+        g = CudaEngine(device=local)
+        g.initGPU()
+        t0 = time.perf_counter()
+        workloads.configure(g, dict(job, probes=[], ade=dict(job["ade"], apply=apply)))
+        g.iterate(1)
+        g.sync()
+        t_cfg = time.perf_counter() - t0
+        stream = torch.cuda.ExternalStream(g.stream)
+        for _ in range(2):
+            g.iterate(100)
+            g.computeEnergy()
+        g.sync()
+        T = max(1, args.dispersive_timesteps // 100) * 100
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(T // 100):
+            g.iterate(100)
+            g.computeEnergy()
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        out = {"timesteps": T, "ms_per_timestep": round(ms / T, 4), "mcells_s": round(N * T / (ms / 1e3) / 1e6, 1),
+               "kernels_per_timestep": g.kernelsPerStep(), "device_gb": round(g.deviceBytes() / 1e9, 2),
+               "host_configure_s": round(t_cfg, 1)}
+        g.destroy()
+        return out
+
+    out = {"workload": "dispersive 800x800x400, UPML8 all faces, Drude/Lorentz spheres 30%, TFSF 30 deg, NF2FF F=5",
+           "cells": N, "dispersive_cells": int(job["dispersive_cells"]), "host_generate_s": round(t_gen, 1)}
+    out.update(run(False))
+    out["ade_applied"] = run(True)
+    # batched form: 16 seeded dispersive solves of 200 x 200 x 100 lines (same
+    # media, UPML, TFSF and NF2FF layout), as the reference's engine runs them
+    if args.dispersive_batch:
+        small = [workloads.dispersive(grid=(200, 200, 100), seed=100 + i, apply=False) for i in range(args.dispersive_batch)]
+        T = 256
+        cells, v_b, v_s, tuned = batch_vs_sequential(small, T, local)
+        out["batched"] = {"workload": "%d dispersive solves 200x200x100" % len(small), "cells": cells,
+                          "timesteps_per_member": T, "batched_mcells_s": round(v_b, 1),
+                          "sequential_mcells_s": round(v_s, 1), "speedup": round(v_b / v_s, 3), "autotuned": tuned}
     return out
 
 
@@ -400,14 +427,21 @@ def served_leg(args, local):
     templates = dict(zip(keys, made))
     prep = time.perf_counter() - t0
 
+    def work(stream):                 # mean cell-steps of one request of the stream
+        return float(np.mean([np.prod(templates[(k, sd)]["grid"]) * steps for _, k, sd, steps in stream]))
+
     def one(stream, members, horizon):
         srv = serve.Server(hbm_budget=150e9, max_members=members, chunk=256, device=local)
         serve.run_stream(stream, templates, srv, horizon=horizon)
         wall = srv.now()
         srv.close()
         done = srv.finished
+        rate = srv.cell_steps / wall
         return {"arrivals": len(stream), "completed": len(done), "wall_s": round(wall, 2),
-                "solves_per_s": round(len(done) / wall, 4), "mcells_s": round(srv.cell_steps / wall / 1e6, 1),
+                "solves_per_s": round(len(done) / wall, 4), "mcells_s": round(rate / 1e6, 1),
+                # completions in a window cut short favour one-at-a-time service; the
+                # steady-state rate is the throughput over the mean request's work
+                "work_equivalent_solves_per_s": round(rate / work(stream), 4),
                 "latency": serve.latency_stats(done), "member_slots": members}
     batched = one(sat, 64, args.served_horizon_s)
     plain = one(sat, 1, args.served_horizon_s)

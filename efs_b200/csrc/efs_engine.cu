@@ -100,7 +100,7 @@ struct efs_engine {
     DevBuf volt, curr;          // fields (parity 0)
     DevBuf volt_b, curr_b;      // second buffers (parity 1): a step reads one parity and writes the other
     int cur = 0;                // parity holding the current fields
-    uint32_t xchunk = 32;       // x-planes per CTA of the fused kernel (EFS_XCHUNK)
+    uint32_t xchunk = 32;       // x-planes per CTA of the fused kernel (efs_set_plane_depth)
     uint64_t wait_ns = 1000000000ull;   // limit of the fused kernel's bounded waits
     uint32_t skip_plane = ~0u;          // diagnostics (efs_debug_set_wait): a plane whose loads are never issued
     DevBuf defer_cells;
@@ -148,17 +148,44 @@ struct efs_engine {
     // buffer in the padded layout (pad cells zero).
     void upload_padded(DevBuf& b, const void* src, size_t comps, size_t elem = 4) {
         alloc(b, comps * Nd * elem, Pz != Nz);
-        ck(cudaMemcpy2DAsync(b.p, (size_t)Pz * elem, src, (size_t)Nz * elem, (size_t)Nz * elem, comps * Nx * Ny,
-                             cudaMemcpyHostToDevice, stream), "upload (padded rows)");
-        sync("upload sync");
+        rows_transfer(b.p, const_cast<void*>(src), comps * Nx * Ny, elem, true);
+    }
+    // Row transfers between the caller's unpadded rows (pitch Nz) in host
+    // memory and the padded device rows (pitch Pz).  Equal pitches: one
+    // linear copy.  Otherwise each chunk of rows crosses PCIe as one linear
+    // copy through a device staging buffer and is repacked by a device-to-
+    // device 2D copy (a 2D copy from pageable host memory moves row by row).
+    // Synchronous with the host on return.
+    void rows_transfer(void* dev, void* host, size_t rows, size_t elem, bool to_device) {
+        const size_t w = (size_t)Nz * elem, dp = (size_t)Pz * elem;
+        if (Pz == Nz) {
+            ck(cudaMemcpyAsync(to_device ? dev : host, to_device ? host : dev, rows * w,
+                               to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, stream), "row transfer");
+            sync("row transfer");
+            return;
+        }
+        const size_t chunk = std::max<size_t>(1, std::min(rows, ((size_t)64 << 20) / w));
+        DevBuf stage;
+        alloc(stage, chunk * w, false);
+        for (size_t r0 = 0; r0 < rows; r0 += chunk) {
+            const size_t n = std::min(chunk, rows - r0);
+            uint8_t* d = static_cast<uint8_t*>(dev) + r0 * dp;
+            uint8_t* h = static_cast<uint8_t*>(host) + r0 * w;
+            if (to_device) {
+                ck(cudaMemcpyAsync(stage.p, h, n * w, cudaMemcpyHostToDevice, stream), "row transfer");
+                ck(cudaMemcpy2DAsync(d, dp, stage.p, w, w, n, cudaMemcpyDeviceToDevice, stream), "row repack");
+            } else {
+                ck(cudaMemcpy2DAsync(stage.p, w, d, dp, w, n, cudaMemcpyDeviceToDevice, stream), "row repack");
+                ck(cudaMemcpyAsync(h, stage.p, n * w, cudaMemcpyDeviceToHost, stream), "row transfer");
+            }
+        }
+        sync("row transfer");   // the staging buffer is freed on return
     }
     void copy_fields_out(float* dst, const float* dev) {
-        ck(cudaMemcpy2DAsync(dst, (size_t)Nz * 4, dev, (size_t)Pz * 4, (size_t)Nz * 4, 3 * (size_t)Nx * Ny,
-                             cudaMemcpyDeviceToHost, stream), "read fields");
+        rows_transfer(const_cast<float*>(dev), dst, 3 * (size_t)Nx * Ny, 4, false);
     }
     void copy_fields_in(float* dev, const float* src) {
-        ck(cudaMemcpy2DAsync(dev, (size_t)Pz * 4, src, (size_t)Nz * 4, (size_t)Nz * 4, 3 * (size_t)Nx * Ny,
-                             cudaMemcpyHostToDevice, stream), "write fields");
+        rows_transfer(dev, const_cast<float*>(src), 3 * (size_t)Nx * Ny, 4, true);
     }
 
     // Mur (host copies kept to rebuild read redirects)
@@ -767,8 +794,6 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     e->h_exc_targets.clear(); e->h_tfsf_v_targets.clear(); e->h_mur_apply.clear(); e->h_rlc_series.clear();
     e->defer_n = 0;
     // plane depth (x-planes per CTA) of the fused kernel; results do not depend on it
-    e->xchunk = 32;
-    if (const char* s = getenv("EFS_XCHUNK")) e->xchunk = std::max(1, atoi(s));
     e->cur = 0;
     e->alloc(e->volt, 3 * Nd * sizeof(float));
     e->alloc(e->curr, 3 * Nd * sizeof(float));
@@ -1734,6 +1759,14 @@ efs_status efs_debug_set_wait(efs_engine* e, uint64_t wait_ns, uint32_t skip_pla
         if (wait_ns == 0 || wait_ns > 10000000000ull) fail(EFS_ERR_INVALID, "wait_ns must be in 1 ns .. 10 s");
         e->wait_ns = wait_ns;
         e->skip_plane = skip_plane;
+        e->dirty();
+    });
+}
+
+efs_status efs_set_plane_depth(efs_engine* e, uint32_t xchunk) {
+    return guard(e, [&] {
+        if (xchunk == 0 || xchunk > 65535) fail(EFS_ERR_INVALID, "plane depth must be in 1 .. 65535");
+        e->xchunk = xchunk;
         e->dirty();
     });
 }

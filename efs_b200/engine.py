@@ -474,6 +474,11 @@ class CudaEngine:
         waits, and an x-plane whose loads are never issued (None: none)."""
         self._ck(self._lib.efs_debug_set_wait(self._h, int(wait_ns), 0xFFFFFFFF if skip_plane is None else int(skip_plane)))
 
+    def setPlaneDepth(self, xchunk):
+        """Tuning (efs_set_plane_depth): x-planes per CTA of the fused kernel
+        (default 32); results are bit-identical under every depth."""
+        self._ck(self._lib.efs_set_plane_depth(self._h, int(xchunk)))
+
     def timeCore(self, reps=10):
         """Mean device ms per launch of [the fused kernel, the UPML passes] (advances the fields)."""
         ms = np.zeros(2, np.float32)

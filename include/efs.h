@@ -308,6 +308,12 @@ efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms);
  * (src/webgpu-engine.mjs:1129-1131). */
 efs_status efs_debug_set_wait(efs_engine* e, uint64_t wait_ns, uint32_t skip_plane);
 
+/* Tuning: x-planes each CTA of the fused kernel streams (default 32; 1 ..
+ * 65535).  Results are bit-identical under every depth; it moves the CTA
+ * seams and trades halo re-reads against parallelism.  Kept across init.
+ * No counterpart in the reference. */
+efs_status efs_set_plane_depth(efs_engine* e, uint32_t xchunk);
+
 /* Diagnostics: kernel launches one timestep enqueues with the current
  * configuration (a captured batch of n steps adds one counter update and,
  * with NF2FF configured, ceil(n/16) accumulator passes). */

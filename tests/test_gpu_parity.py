@@ -18,19 +18,28 @@ from oracle.oracle import OracleEngine, far_field
 
 pytestmark = pytest.mark.gpu
 
-# Plane depth of the fused kernel: the default, and 3 x-planes per CTA so that
-# CTA seams fall inside the test grids (results must not depend on it).
+# Plane depth of the fused kernel (efs_set_plane_depth): the default, and 3
+# x-planes per CTA so that CTA seams fall inside the test grids (results must
+# not depend on it).
 CORES = {
-    "fused": {},
-    "fused_x3": {"EFS_XCHUNK": "3"},
+    "fused": None,
+    "fused_x3": 3,
 }
 
 
 @pytest.fixture(autouse=True, params=list(CORES))
 def core_path(request, monkeypatch):
-    monkeypatch.delenv("EFS_XCHUNK", raising=False)
-    for k, v in CORES[request.param].items():
-        monkeypatch.setenv(k, v)
+    depth = CORES[request.param]
+    if depth is not None:
+        from efs_b200.engine import CudaEngine
+        init_gpu = CudaEngine.initGPU
+
+        def initGPU(self, *a, **k):
+            ok = init_gpu(self, *a, **k)
+            if ok:
+                self.setPlaneDepth(depth)
+            return ok
+        monkeypatch.setattr(CudaEngine, "initGPU", initGPU)
     return request.param
 
 
@@ -146,6 +155,36 @@ def test_pml_bitexact(cuda_engine_cls, overlap):
     g.iterate(25)
     o.iterate(25)
     compare_fields(g, o, "pml")
+    for r in range(len(regs)):
+        assert_bitexact(g.debugRead("pml_volt_flux", r), o.read("pml_volt_flux", r), "vflux %d" % r)
+        assert_bitexact(g.debugRead("pml_curr_flux", r), o.read("pml_curr_flux", r), "cflux %d" % r)
+
+
+# 8-cell z-slab regions are updated inside the fused kernel from TMA-staged flux
+# (a slab overlapping other regions keeps its shared cells in the UPML passes)
+ZSLAB_CASES = {
+    "z_only": ((20, 23, 50), [((0, 0, 0), (20, 23, 8)), ((0, 0, 42), (20, 23, 8))]),
+    "six_faces": ((24, 22, 40), [((0, 0, 0), (8, 22, 40)), ((16, 0, 0), (8, 22, 40)), ((0, 0, 0), (24, 8, 40)),
+                                 ((0, 14, 0), (24, 8, 40)), ((0, 0, 0), (24, 22, 8)), ((0, 0, 32), (24, 22, 8))]),
+    "both_in_one_tile": ((12, 17, 20), [((0, 0, 0), (12, 17, 8)), ((0, 0, 12), (12, 17, 8))]),
+    "partial_rows": ((14, 21, 37), [((2, 3, 0), (8, 11, 8)), ((0, 9, 29), (14, 12, 8)), ((5, 0, 10), (6, 21, 8))]),
+}
+
+
+@pytest.mark.parametrize("indexed", [False, True])
+@pytest.mark.parametrize("case", list(ZSLAB_CASES))
+def test_pml_zslab_bitexact(cuda_engine_cls, case, indexed):
+    N, boxes = ZSLAB_CASES[case]
+    c = rand_coeffs(N, 21) if not indexed else free_space(*N)
+    g, o = both(cuda_engine_cls, N, c, indexed)
+    regs = [pml_region(s, n, 60 + i) for i, (s, n) in enumerate(boxes)]
+    for e in (g, o):
+        e.configurePML(regs)
+    seed_fields(g, o, N, 22)
+    for steps in (1, 6, 23):
+        g.iterate(steps)
+        o.iterate(steps)
+        compare_fields(g, o, "zslab %s +%d" % (case, steps))
     for r in range(len(regs)):
         assert_bitexact(g.debugRead("pml_volt_flux", r), o.read("pml_volt_flux", r), "vflux %d" % r)
         assert_bitexact(g.debugRead("pml_curr_flux", r), o.read("pml_curr_flux", r), "cflux %d" % r)
