@@ -207,6 +207,7 @@ def batch_vs_sequential(jobs, T, local):
     cells = sum(j["grid"][0] * j["grid"][1] * j["grid"][2] for j in jobs)
     b = CudaBatch(engines)
     tuned = b.autotune(steps=8)                  # real timesteps, identical results under every shape
+    tuned["phases_ms"] = b.timePhases(32)        # per-phase device ms per batched timestep
     b.iterate(T)
     b.sync()
     t0 = time.perf_counter()
@@ -378,7 +379,7 @@ def dispersive_leg(args, local):
         ms = ev0.elapsed_time(ev1)
         out = {"timesteps": T, "ms_per_timestep": round(ms / T, 4), "mcells_s": round(N * T / (ms / 1e3) / 1e6, 1),
                "kernels_per_timestep": g.kernelsPerStep(), "device_gb": round(g.deviceBytes() / 1e9, 2),
-               "host_configure_s": round(t_cfg, 1)}
+               "host_configure_s": round(t_cfg, 1), "phases_ms": g.timePhases(16)}
         g.destroy()
         return out
 
@@ -522,6 +523,7 @@ def run_b200(args):
     chunks = [64] * (BATCH // 64) + ([BATCH % 64] if BATCH % 64 else [])
     nf_passes = sum(math.ceil(m / 16) for m in chunks) if job.get("nf2ff") else 0
     launches = args.steps * (BATCH * eng.kernelsPerStep() + len(chunks) + nf_passes + 2)
+    phases = eng.timePhases(32)              # per-phase device ms per timestep, launched kernel by kernel
     far = None
     if rank == 0 and world == 1 and not args.no_far_field and job.get("nf2ff"):
         far = far_field_leg(eng, job, local)
@@ -540,9 +542,13 @@ def run_b200(args):
         g = CudaEngine(device=local)
         g.initGPU()
         workloads.configure(g, dict(job, probes=[]))
+        g.sync()
+        t1 = time.perf_counter()
         for _ in range(args.steps):
             g.iterate(BATCH)
             g.computeEnergy()
+        g.sync()
+        t2 = time.perf_counter()
         acc = g.readNF2FFAccumulation(True)
         en = g.flushEnergy()
         g.destroy()
@@ -550,7 +556,8 @@ def run_b200(args):
         d2h = (acc["accumE"].nbytes + acc["accumH"].nbytes + 8 * (args.steps + 1)) if acc else 8 * args.steps
         e2e = {"value": round(N * steps_total / dt / 1e6, 3), "unit": "MCells/s",
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
-               "wall_s": round(dt, 3)}
+               "wall_s": round(dt, 3), "setup_s": round(t1 - t0, 3), "run_s": round(t2 - t1, 3),
+               "readback_s": round(dt - (t2 - t0), 3)}
         del en
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -584,6 +591,7 @@ def run_b200(args):
                               "unit": "GB/s", "frac": round(step_bytes / (ms_max / steps_total / 1e3) / 1e9 / peak, 4),
                               "what": "whole timestep (all kernels) against its algorithmic bytes"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "phases_ms": phases,
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "batched": batched,

@@ -92,6 +92,8 @@ SIGNATURES = {
     "efs_device_bytes": (C.c_int, [vp, C.POINTER(szt)]),
     "efs_debug_read": (C.c_int, [vp, C.c_char_p, u32, f32p, szt, C.POINTER(szt)]),
     "efs_time_core": (C.c_int, [vp, u32, f32p]),
+    "efs_time_phases": (C.c_int, [vp, u32, f32p]),
+    "efs_batch_time_phases": (C.c_int, [vp, u32, f32p]),
     "efs_debug_set_wait": (C.c_int, [vp, C.c_uint64, u32]),
     "efs_set_plane_depth": (C.c_int, [vp, u32]),
     "efs_kernels_per_step": (C.c_int, [vp, u32p]),

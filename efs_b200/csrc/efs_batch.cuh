@@ -108,9 +108,9 @@ struct OpNfFlush {
 };
 template <bool IDX>
 struct OpDeferred {
-    FusedGrid g; PmlSet ps, pn; const uint32_t* cells; uint32_t n;
+    FusedGrid g; const uint32_t* cells; uint32_t n;
     __device__ void run(uint32_t blk, uint32_t, uint32_t, uint32_t) const {
-        deferred_h_body<IDX, true>(g, ps, pn, cells, n, blk * blockDim.x + threadIdx.x);
+        deferred_h_body<IDX>(g, cells, n, blk * blockDim.x + threadIdx.x);
     }
 };
 template <bool IDX>
@@ -300,8 +300,8 @@ struct efs_batch {
                     any_nf = true;
                 }
                 if (e->defer_n) {
-                    if (e->indexed) vdi.push_back({e->defer_n, OpDeferred<true>{fg, ps, pn, e->defer_cells.as<uint32_t>(), e->defer_n}});
-                    else vdd.push_back({e->defer_n, OpDeferred<false>{fg, ps, pn, e->defer_cells.as<uint32_t>(), e->defer_n}});
+                    if (e->indexed) vdi.push_back({e->defer_n, OpDeferred<true>{fg, e->defer_cells.as<uint32_t>(), e->defer_n}});
+                    else vdd.push_back({e->defer_n, OpDeferred<false>{fg, e->defer_cells.as<uint32_t>(), e->defer_n}});
                 }
                 if (e->pml_split()) {
                     const uint32_t it = e->pml_items();
@@ -358,12 +358,17 @@ struct efs_batch {
     }
 
     // Timestep k of a captured batch at step phase s: the single engine's phase order, each phase for all members.
-    void enqueue_step(uint32_t k, int s, bool last) {
+    // marks: optional EFS_PHASES + 1 phase-boundary events (efs_batch_time_phases).
+    void enqueue_step(uint32_t k, int s, bool last, cudaEvent_t* marks = nullptr) {
+        auto mark = [&](int i) { if (marks) ck(cudaEventRecord(marks[i], stream), "phase mark"); };
+        mark(0);
+        launch_seg<OpPmlE<true>>(pml_e_i[s], k);  // UPML E (the pre-update reads of UPML cells are redirected
+        launch_seg<OpPmlE<false>>(pml_e_d[s], k); // to the old flux, which this pass does not write)
+        mark(1);
         launch_seg<OpAde>(ade_v[s], k);          // pre-voltage, as the single engine: ADE(volt), Mur pre
         launch_seg<OpMurPre>(mur_pre[s], k);
         launch_seg<OpAde>(ade_c[s], k);          // ADE(curr) before the core update rewrites H and the flux
-        launch_seg<OpPmlE<true>>(pml_e_i[s], k);
-        launch_seg<OpPmlE<false>>(pml_e_d[s], k);
+        mark(2);
         const BatchMember* bm = members[s].as<BatchMember>();
         if (ntiles[1])
             k_fused_tma_batch<true><<<std::min<uint32_t>(ntiles[1], ctas_per_sm * sms), TT_THREADS, TT_SMEM_BYTES, stream>>>(
@@ -371,23 +376,64 @@ struct efs_batch {
         if (ntiles[0])
             k_fused_tma_batch<false><<<std::min<uint32_t>(ntiles[0], ctas_per_sm * sms), TT_THREADS, TT_SMEM_BYTES, stream>>>(
                 bm, tiles[0].as<BatchTile>(), ntiles[0]);
-        launch_seg<OpPmlH<true>>(pml_h_i[s], k);
-        launch_seg<OpPmlH<false>>(pml_h_d[s], k);
+        mark(3);
         launch_seg<OpPoints<1>>(tfsf_v[s], k);
         launch_seg<OpMurPost>(mur_post[s], k);
         launch_seg<OpPoints<0>>(exc[s], k);
         launch_seg<OpMurApply>(mur_apply[s], k);
         launch_seg<OpAdeApply>(ade_apply_v[s], k);
+        mark(4);
+        launch_seg<OpPmlH<true>>(pml_h_i[s], k);       // UPML H after the E-side operations (no deferred
+        launch_seg<OpPmlH<false>>(pml_h_d[s], k);      // cell is a UPML cell)
         launch_seg<OpDeferred<true>>(deferred_i[s], k);
         launch_seg<OpDeferred<false>>(deferred_d[s], k);
+        mark(5);
         launch_seg<OpPoints<1>>(tfsf_c[s], k);
         launch_seg<OpAdeApply>(ade_apply_c[s], k);
+        mark(6);
         if (any_nf) {
             const uint32_t j = k % NF_K;
             launch_seg<OpNfSample>(nf_sample[s], k, j);
             if (j == NF_K - 1 || last) launch_seg<OpNfFlush>(nf_flush[s], k, k - j, j + 1);
         }
         launch_seg<OpRing>(ring[s], k);
+        mark(7);
+    }
+    // `steps` (<= 64) timesteps launched one kernel at a time with phase marks;
+    // accumulates device ms per phase into ms[EFS_PHASES] (same results as iterate).
+    void run_marked(uint32_t steps, float* ms) {
+        if (stale()) plan();
+        for (size_t i = 0; i < mem.size(); ++i) {
+            ck(cudaEventRecord(ev_in[i], mem[i]->stream), "event");
+            ck(cudaStreamWaitEvent(stream, ev_in[i], 0), "wait");
+        }
+        std::vector<cudaEvent_t> ev((size_t)steps * (EFS_PHASES + 1));
+        for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+        try {
+            for (uint32_t k = 0; k < steps; ++k)
+                enqueue_step(k, (int)((phase + k) & 1), k + 1 == steps, ev.data() + (size_t)k * (EFS_PHASES + 1));
+            launch_seg<OpAdvance>(advance, 0, steps);
+            ck(cudaGetLastError(), "batch phase run");
+            ck(cudaStreamSynchronize(stream), "batch phase run");
+            for (uint32_t k = 0; k < steps; ++k)
+                for (int i = 0; i < EFS_PHASES; ++i) {
+                    float t = 0;
+                    const size_t b = (size_t)k * (EFS_PHASES + 1) + i;
+                    ck(cudaEventElapsedTime(&t, ev[b], ev[b + 1]), "elapsed");
+                    ms[i] += t;
+                }
+        } catch (...) {
+            for (auto& x : ev) cudaEventDestroy(x);
+            throw;
+        }
+        for (auto& x : ev) cudaEventDestroy(x);
+        for (efs_engine* e : mem) {
+            e->numTS += steps;
+            if (steps & 1) e->cur ^= 1;
+        }
+        if (steps & 1) phase ^= 1;
+        ck(cudaEventRecord(ev_done, stream), "event");
+        for (efs_engine* e : mem) ck(cudaStreamWaitEvent(e->stream, ev_done, 0), "wait");
     }
 
     cudaGraphExec_t graph_for(uint32_t m) {
@@ -529,6 +575,15 @@ efs_status efs_batch_set_shape(efs_batch* b, uint32_t xchunk, uint32_t ctas_per_
         b->xchunk = xchunk;
         if (ctas_per_sm != b->ctas_per_sm) b->drop_graphs();
         b->ctas_per_sm = ctas_per_sm;
+    });
+}
+
+efs_status efs_batch_time_phases(efs_batch* b, uint32_t steps, float* ms) {
+    return bguard(b, [&] {
+        if (!ms || steps == 0 || steps > 64) fail(EFS_ERR_INVALID, "ms must be non-null and steps in 1..64");
+        for (int i = 0; i < EFS_PHASES; ++i) ms[i] = 0.f;
+        b->run_marked(steps, ms);
+        for (int i = 0; i < EFS_PHASES; ++i) ms[i] /= (float)steps;
     });
 }
 

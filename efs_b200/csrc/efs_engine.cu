@@ -247,6 +247,7 @@ struct efs_engine {
     uint32_t gd_n = 0;
     bool ring_on = false;
     DevBuf ring_idx, ring;
+    std::vector<uint32_t> h_nf_pts;   // host copy of the NF2FF points (plan checks)
     uint32_t ring_n = 0, ring_max = 0, ring_interval = 1, ring_q0 = 0;
 
     // NF2FF
@@ -389,6 +390,7 @@ struct efs_engine {
     // Rebuild everything that depends on more than one configure call.
     void build_plan() {
         if (!plan_dirty) return;
+        nf_pair = nf2ff_clear_of_pml();
         for (int p = 0; p < 2; ++p) {
             std::vector<float*> vp, cp;
             for (auto& r : pml) { vp.push_back(r->vf(p)); cp.push_back(r->cf(p)); }
@@ -520,20 +522,51 @@ struct efs_engine {
             if (n != 1) mark(x, y - 1, z);
             if (n != 2) mark(x, y, z - 1);
         }
+        // UPML cells are left to k_pml_h, which runs after the E-side operations
+        for (auto& R : pml)
+            for (uint32_t x = R->s[0]; x < R->s[0] + R->n[0]; ++x)
+                for (uint32_t y = R->s[1]; y < R->s[1] + R->n[1]; ++y)
+                    for (uint32_t z = R->s[2]; z < R->s[2] + R->n[2]; ++z) {
+                        const size_t c = dev_cell(x, y, z);
+                        bits[c >> 5] &= ~(1u << (c & 31));
+                    }
         std::vector<uint32_t> cells;
         for (size_t w = 0; w < bits.size(); ++w)
             for (uint32_t b = bits[w]; b; b &= b - 1) cells.push_back((uint32_t)(w * 32 + __builtin_ctz(b)));
         upload(defer_cells, cells);
         defer_n = (uint32_t)cells.size();
     }
+    // The NF2FF samples of a step may run beside the next step's UPML E pass
+    // when no sample interpolates over a UPML cell (the only cells of its
+    // inputs that pass rewrites in place).
+    bool nf2ff_clear_of_pml() const {
+        if (!nf_on) return false;
+        for (size_t i = 0; i + 2 < h_nf_pts.size(); i += 3) {
+            const uint32_t x = h_nf_pts[i], y = h_nf_pts[i + 1], z = h_nf_pts[i + 2];   // cells (x..x+1, y..y+1, z..z+1)
+            for (auto& R : pml)
+                if (x < R->s[0] + R->n[0] && R->s[0] <= x + 1 && y < R->s[1] + R->n[1] && R->s[1] <= y + 1 &&
+                    z < R->s[2] + R->n[2] && R->s[2] <= z + 1)
+                    return false;
+        }
+        return true;
+    }
 
     // Enqueue timestep k of a batch (numTS = state.numTS + k); the fields are
     // read from parity p and written to parity 1 - p.
     // `last`: k is the batch's final step (buffered NF2FF samples are flushed).
-    void enqueue_step(uint32_t k, int p, bool last) {
+    // marks: optional EFS_PHASES + 1 events recorded at the phase boundaries
+    // (efs_time_phases); null inside captured graphs.
+    //
+    // Latency-bound passes are paired into one launch (k_pair): the UPML H
+    // pass with the deferred H (both after the E-side point operations; no
+    // deferred cell is a UPML cell), and, when no NF2FF sample reads a UPML
+    // cell (plan flag nf_pair), a step's NF2FF samples with the next step's
+    // UPML E pass (k_pml_e rewrites only UPML cells of those inputs, in place);
+    // the samples of a batch's last step run on their own.
+    void enqueue_step(uint32_t k, int p, bool last, cudaEvent_t* marks = nullptr) {
+        auto mark = [&](int i) { if (marks) ck(cudaEventRecord(marks[i], stream), "phase mark"); };
+        mark(0);
         const int q = pnext(p);
-        const PmlSet ps = pml_set(p);
-        const PmlSet pn = pml_set(q);
         StepState* st = state.as<StepState>();
         float* V = vbuf(p);          // E before the core update
         float* C = cbuf(p);          // H before the core update
@@ -542,23 +575,34 @@ struct efs_engine {
         const uint32_t T = 256;
         const float* const* vfl = vflux_ptrs[p].as<const float*>();
         const float* const* cfl = cflux_ptrs[p].as<const float*>();
+        const bool split = pml_split();
 
         // --- pre-voltage ---
-        if (ss_on)
+        if (ss_on)     // reads the fields before the UPML pre-update
             k_steady_state<<<blocks(ss_n, T), T, 0, stream>>>(V, st, k, ss_idx.as<uint32_t>(), ss_n, ss_period,
                                                               ss_e1.as<float>(), ss_e2.as<float>());
+        if (nf_held.on) {            // samples of step k-1 (its fields are this step's inputs) beside the UPML E pass
+            const PassNfSample a{V, C, nf_held.j, nf};
+            const uint32_t na = blocks(nf.np, T), nb = blocks(pml_items(), T);
+            if (indexed) pair(a, na, pml_e_pass<true>(p), nb);
+            else pair(a, na, pml_e_pass<false>(p), nb);
+            if (nf_held.j == NF_K - 1) k_nf2ff_flush<<<blocks(nf.np, T), T, 0, stream>>>(st, k - 1 - nf_held.j, nf_held.j + 1, nf);
+            nf_held.on = false;
+        } else if (split) {
+            launch_pml_e(p);
+        }
+        mark(1);
         if (ade_v.live()) k_ade<<<blocks(ade_v.n, ADE_BLOCK), ADE_T, 0, stream>>>(V, ade_dev(ade_v, vfl));
         MurDev md = mur_dev(vfl);
         if (mur_on) k_mur_pre<<<blocks(mur_n, T), T, 0, stream>>>(V, md);
         RlcDev rd = rlc_dev();
         if (rlc_on) k_rlc_pre<<<blocks(rlc_n, T), T, 0, stream>>>(rd);
-        const bool hp = !pml.empty();
         // ADE(curr) reads H and the current flux, which the E side never
         // touches: it runs before the fused kernel overwrites the flux.
         if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
-        if (hp) launch_pml_e(p);
+        mark(2);
         launch_fused_tma(p);
-        if (hp) launch_pml_h(p);
+        mark(3);
         // --- post-voltage / apply (on the updated E) ---
         if (tfsf_on && tfsf_v.groups) k_point_sources<1><<<blocks(tfsf_v.groups, T), T, 0, stream>>>(V1, st, k, point_dev(tfsf_v, tfsf_signal, tfsf_len, tfsf_period));
         if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, true, V1);
@@ -571,25 +615,89 @@ struct efs_engine {
         if (mur_on) k_mur_apply<<<blocks(mur_napply, T), T, 0, stream>>>(V1, md);
         if (rlc_on) k_rlc_apply<<<blocks(rlc_groups, T), T, 0, stream>>>(V1, rd);
         if (ade_apply && ade_v.live()) launch_ade_apply(ade_v, V1);
-        if (defer_n) {
-            const FusedGrid fg = fused_grid(p);
-            const uint32_t* cells = defer_cells.as<uint32_t>();
-            if (indexed) { if (hp) k_deferred_h<true, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<true, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
-            else { if (hp) k_deferred_h<false, true><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); else k_deferred_h<false, false><<<blocks(defer_n, T), T, 0, stream>>>(fg, ps, pn, cells, defer_n); }
-        }
+        mark(4);
+        // --- H of the UPML cells and of the cells next to those E writes ---
+        if (split && defer_n) {
+            const uint32_t na = blocks(pml_items(), T), nb = blocks(defer_n, T);
+            if (indexed) pair(pml_h_pass<true>(p), na, deferred_pass<true>(p), nb);
+            else pair(pml_h_pass<false>(p), na, deferred_pass<false>(p), nb);
+        } else if (split) launch_pml_h(p);
+        else if (defer_n) launch_deferred(p);
+        mark(5);
         // --- post-current (on the updated H) ---
         if (tfsf_on && tfsf_c.groups) k_point_sources<1><<<blocks(tfsf_c.groups, T), T, 0, stream>>>(C1, st, k, point_dev(tfsf_c, tfsf_signal, tfsf_len, tfsf_period));
         if (pbc_on) for (auto& a : pbc_axes) launch_pbc(a, false, C1);
         if (ade_apply && ade_c.live()) launch_ade_apply(ade_c, C1);
+        mark(6);
         // --- after the step ---
         if (nf_on) {
             // surface samples of this step; the accumulators take every NF_K steps
             // and the batch's last step (nothing stays pending between batches)
             const uint32_t j = k % NF_K;
-            k_nf2ff_sample<<<blocks(nf.np, T), T, 0, stream>>>(V1, C1, j, nf);
-            if (j == NF_K - 1 || last) k_nf2ff_flush<<<blocks(nf.np, T), T, 0, stream>>>(st, k - j, j + 1, nf);
+            if (nf_pair && split && !last) {
+                nf_held = NfHeld{true, j};           // sampled beside the next step's UPML E pass
+            } else {
+                k_nf2ff_sample<<<blocks(nf.np, T), T, 0, stream>>>(V1, C1, j, nf);
+                if (j == NF_K - 1 || last) k_nf2ff_flush<<<blocks(nf.np, T), T, 0, stream>>>(st, k - j, j + 1, nf);
+            }
         }
         if (ring_on) k_gather_ring<<<blocks(ring_n, 64), 64, 0, stream>>>(V1, C1, st, k, ring_dev());
+        mark(7);
+    }
+    struct NfHeld { bool on; uint32_t j; };
+    NfHeld nf_held{false, 0};     // capture: NF2FF samples of the previous step not yet issued
+    bool nf_pair = false;         // plan: no NF2FF sample reads a UPML cell
+    // passes of the paired launches (k_pair, 256-thread blocks)
+    template <bool IDX> PassPmlE<IDX> pml_e_pass(int p) const {
+        return PassPmlE<IDX>{fused_grid(p), pml_set(p), pml_set(1 - p), vbuf(p), pml_items()};
+    }
+    template <bool IDX> PassPmlH<IDX> pml_h_pass(int p) const {
+        return PassPmlH<IDX>{fused_grid(p), pml_set(p), pml_set(1 - p), pml_items()};
+    }
+    template <bool IDX> PassDeferred<IDX> deferred_pass(int p) const {
+        return PassDeferred<IDX>{fused_grid(p), defer_cells.as<uint32_t>(), defer_n};
+    }
+    template <class A, class B>
+    void pair(const A& a, uint32_t na, const B& b, uint32_t nb) {
+        if (na + nb) k_pair<A, B><<<na + nb, 256, 0, stream>>>(a, na, b, nb);
+    }
+    void launch_deferred(int p) {
+        const uint32_t T = 256;
+        if (indexed) k_deferred_h<true><<<blocks(defer_n, T), T, 0, stream>>>(fused_grid(p), defer_cells.as<uint32_t>(), defer_n);
+        else k_deferred_h<false><<<blocks(defer_n, T), T, 0, stream>>>(fused_grid(p), defer_cells.as<uint32_t>(), defer_n);
+    }
+    // `steps` timesteps (at most 64) launched one kernel at a time with the
+    // phase marks; accumulates device ms per phase into ms[EFS_PHASES].  Same
+    // results as iterate(steps).
+    void run_marked(uint32_t steps, float* ms) {
+        need_init();
+        build_plan();
+        std::vector<cudaEvent_t> ev((size_t)steps * (EFS_PHASES + 1));
+        for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+        nf_held.on = false;
+        try {
+            int q = cur;
+            for (uint32_t k = 0; k < steps; ++k) {
+                enqueue_step(k, q, k + 1 == steps, ev.data() + (size_t)k * (EFS_PHASES + 1));
+                q = pnext(q);
+            }
+            k_advance<<<1, 1, 0, stream>>>(state.as<StepState>(), steps);
+            ck(cudaGetLastError(), "phase run");
+            sync("phase run");
+            for (uint32_t k = 0; k < steps; ++k)
+                for (int i = 0; i < EFS_PHASES; ++i) {
+                    float t = 0;
+                    const size_t b = (size_t)k * (EFS_PHASES + 1) + i;
+                    ck(cudaEventElapsedTime(&t, ev[b], ev[b + 1]), "elapsed");
+                    ms[i] += t;
+                }
+        } catch (...) {
+            for (auto& x : ev) cudaEventDestroy(x);
+            throw;
+        }
+        for (auto& x : ev) cudaEventDestroy(x);
+        numTS += steps;
+        if (steps & 1) cur ^= 1;
     }
     RingDev ring_dev() const { return RingDev{ring_idx.as<uint32_t>(), ring_n, ring_interval, ring_q0, ring_max, ring.as<float>()}; }
 
@@ -714,6 +822,7 @@ struct efs_engine {
         if (graphs.size() > 12) drop_graphs();
         cudaGraph_t graph;
         ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "BeginCapture");
+        nf_held.on = false;
         try {
             int q = p;
             for (uint32_t k = 0; k < m; ++k) { enqueue_step(k, q, k + 1 == m); q = pnext(q); }
@@ -1377,6 +1486,7 @@ efs_status efs_configure_nf2ff(efs_engine* e, const uint32_t* pts, uint32_t np, 
         for (uint32_t i = 0; i < np; ++i)
             if (pts[3 * i] >= e->Nx || pts[3 * i + 1] >= e->Ny || pts[3 * i + 2] >= e->Nz) fail(EFS_ERR_INVALID, "NF2FF point out of grid");
         e->upload(e->nf_pts, pts, 3 * (size_t)np);
+        e->h_nf_pts.assign(pts, pts + 3 * (size_t)np);
         size_t nel = 2 * ((size_t)e->Nx + e->Ny + e->Nz);
         e->upload(e->nf_el, el, nel);
         e->alloc(e->nf_E, (size_t)nf * np * 6 * 4);
@@ -1801,17 +1911,27 @@ efs_status efs_time_core(efs_engine* e, uint32_t reps, float* ms) {
     });
 }
 
+efs_status efs_time_phases(efs_engine* e, uint32_t steps, float* ms) {
+    return guard(e, [&] {
+        if (!ms || steps == 0 || steps > 64) fail(EFS_ERR_INVALID, "ms must be non-null and steps in 1..64");
+        for (int i = 0; i < EFS_PHASES; ++i) ms[i] = 0.f;
+        e->run_marked(steps, ms);
+        for (int i = 0; i < EFS_PHASES; ++i) ms[i] /= (float)steps;
+    });
+}
+
 efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out) {
     return guard(e, [&] {
         e->need_init();
         if (!out) fail(EFS_ERR_INVALID, "out must be non-null");
         e->build_plan();
-        uint32_t k = 1 + (e->defer_n > 0) + 2 * e->pml_split();   // fused kernel (+ deferred H, UPML passes)
+        // fused kernel, UPML E pass, UPML H pass and deferred H (one paired launch when both)
+        uint32_t k = 1 + e->pml_split() + ((e->defer_n > 0) || e->pml_split());
         k += e->ss_on + e->ade_v.live() + e->ade_c.live() + 3 * e->mur_on + 2 * e->rlc_on;
         if (e->ade_apply) k += e->ade_v.live() + e->ade_c.live();
         k += (e->tfsf_on && e->tfsf_v.groups) + (e->tfsf_on && e->tfsf_c.groups) + (e->exc_on && e->exc_groups > 0);
         k += e->pbc_on ? 2 * (uint32_t)e->pbc_axes.size() : 0;
-        k += e->nf_on + e->ring_on;
+        k += (e->nf_on && !(e->nf_pair && e->pml_split())) + e->ring_on;   // paired samples ride on the UPML E pass
         *out = k;
     });
 }

@@ -16,7 +16,8 @@
 // H cells whose curl reads an E value that a sparse post-update operation
 // rewrites (TFSF, Mur apply, excitation, PBC, series RLC, the ADE apply step)
 // get a provisional H from the fused kernel and are recomputed by
-// k_deferred_h, which runs after those operations.  The result is the
+// k_deferred_h, which runs after those operations (UPML cells among them are
+// left to k_pml_h, which runs after them as well).  The result is the
 // reference's phase order exactly, bit for bit.
 #pragma once
 #include "efs_kernels.cuh"
@@ -104,11 +105,12 @@ __device__ __forceinline__ void coeffs_f(const FusedGrid& g, size_t c, uint32_t 
     }
 }
 
-// H update of the deferred cells, after the E-side sparse operations:
-// reads the final E_new, H_old, writes H_new (with UPML), one thread per cell.
-template <bool IDX, bool PML>
-__device__ __forceinline__ void deferred_h_body(const FusedGrid& g, const PmlSet& ps, const PmlSet& pn, const uint32_t* cells,
-                                                uint32_t n, uint32_t i) {
+// H update of the deferred cells, after the E-side sparse operations: reads
+// the final E_new and H_old, writes H_new, one thread per cell.  No deferred
+// cell is a UPML cell (k_pml_h, which runs after the E-side operations too,
+// updates those).
+template <bool IDX>
+__device__ __forceinline__ void deferred_h_body(const FusedGrid& g, const uint32_t* cells, uint32_t n, uint32_t i) {
     if (i >= n) return;
     const uint32_t c = cells[i];
     const uint32_t N = (uint32_t)g.N, NyNz = (uint32_t)g.NyNz, Pz = g.Pz;   // 3*N < 2^32
@@ -133,18 +135,11 @@ __device__ __forceinline__ void deferred_h_body(const FusedGrid& g, const PmlSet
         coeffs_f<IDX>(g, c, m, 6, kk);
     }
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        float hn;
-        if (PML) hn = pml_chain_pp<false>(ps, pn, ps.count >= 32 ? ~0u : ((1u << ps.count) - 1u), x, y, z, q, ho[q], core,
-                                          kk[q], kk[3 + q], cv[q], true);
-        else hn = core ? upd(ho[q], kk[q], kk[3 + q], cv[q]) : ho[q];
-        g.H1[q * N + c] = hn;
-    }
+    for (int q = 0; q < 3; ++q) g.H1[q * N + c] = core ? upd(ho[q], kk[q], kk[3 + q], cv[q]) : ho[q];
 }
-template <bool IDX, bool PML>
-__global__ void __launch_bounds__(256) k_deferred_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, const uint32_t* cells,
-                                                    uint32_t n) {
-    deferred_h_body<IDX, PML>(g, ps, pn, cells, n, blockIdx.x * blockDim.x + threadIdx.x);
+template <bool IDX>
+__global__ void __launch_bounds__(256) k_deferred_h(const FusedGrid g, const uint32_t* cells, uint32_t n) {
+    deferred_h_body<IDX>(g, cells, n, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace efs

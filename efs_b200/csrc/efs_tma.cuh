@@ -512,8 +512,8 @@ __global__ void __launch_bounds__(256, PML_MINB) k_pml_e(const FusedGrid g, cons
     pml_e_body<IDX>(g, ps, pn, V0w, items, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// H_new of the UPML cells from the final-core E_new (cells whose curl reads E
-// rewritten by a sparse operation are redone by k_deferred_h).
+// H_new of the UPML cells from the final E_new: runs after the E-side point
+// operations (beside k_deferred_h, which leaves UPML cells to this pass).
 template <bool IDX>
 __device__ __forceinline__ void pml_h_body(const FusedGrid& g, const PmlSet& ps, const PmlSet& pn, uint32_t items, uint32_t i) {
     if (i >= items) return;
@@ -577,6 +577,46 @@ __device__ __forceinline__ void pml_h_body(const FusedGrid& g, const PmlSet& ps,
 template <bool IDX>
 __global__ void __launch_bounds__(256, PML_MINB) k_pml_h(const FusedGrid g, const PmlSet ps, const PmlSet pn, uint32_t items) {
     pml_h_body<IDX>(g, ps, pn, items, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Two independent passes in one launch.  The UPML passes, the deferred H and
+// the NF2FF samples are latency-bound (40-56% of DRAM bandwidth alone: their
+// items sit one or two per z row); launched as one grid with their blocks
+// interleaved, each pass's loads overlap the other's.  Block i: while both
+// passes have blocks left, even blocks run A and odd blocks run B; the rest
+// run the longer pass.  Every pass uses 256-thread blocks.
+// ---------------------------------------------------------------------------
+template <bool IDX>
+struct PassPmlE {
+    FusedGrid g; PmlSet ps, pn; float* V0w; uint32_t items;
+    __device__ void run(uint32_t blk) const { pml_e_body<IDX>(g, ps, pn, V0w, items, blk * 256u + threadIdx.x); }
+};
+template <bool IDX>
+struct PassPmlH {
+    FusedGrid g; PmlSet ps, pn; uint32_t items;
+    __device__ void run(uint32_t blk) const { pml_h_body<IDX>(g, ps, pn, items, blk * 256u + threadIdx.x); }
+};
+template <bool IDX>
+struct PassDeferred {
+    FusedGrid g; const uint32_t* cells; uint32_t n;
+    __device__ void run(uint32_t blk) const { deferred_h_body<IDX>(g, cells, n, blk * 256u + threadIdx.x); }
+};
+struct PassNfSample {
+    const float* V; const float* C; uint32_t slot; Nf2ffDev d;
+    __device__ void run(uint32_t blk) const { nf2ff_sample_body(V, C, slot, d, blk * 256u + threadIdx.x); }
+};
+template <class A, class B>
+__global__ void __launch_bounds__(256, PML_MINB) k_pair(const A a, uint32_t na, const B b, uint32_t nb) {
+    const uint32_t i = blockIdx.x, m = min(na, nb);
+    if (i < 2 * m) {
+        if (i & 1u) b.run(i >> 1);
+        else a.run(i >> 1);
+    } else if (na > nb) {
+        a.run(i - m);
+    } else {
+        b.run(i - m);
+    }
 }
 
 }  // namespace efs

@@ -17,6 +17,9 @@ import numpy as np
 from . import _lib
 from ._lib import EfsError
 
+# Phases of a timestep as efs_time_phases / efs_batch_time_phases report them (EFS_PHASES)
+PHASES = ("upml_e", "pre_point_ops", "core", "e_point_ops", "upml_h_deferred_h", "h_point_ops", "outputs")
+
 __all__ = ["CudaEngine", "EfsError"]
 
 
@@ -474,6 +477,14 @@ class CudaEngine:
         waits, and an x-plane whose loads are never issued (None: none)."""
         self._ck(self._lib.efs_debug_set_wait(self._h, int(wait_ns), 0xFFFFFFFF if skip_plane is None else int(skip_plane)))
 
+    def timePhases(self, steps=16):
+        """Diagnostics (efs_time_phases): device ms per timestep of each phase
+        of the step over `steps` (<= 64) timesteps launched kernel by kernel
+        (advances the engine as iterate does)."""
+        ms = (C.c_float * len(PHASES))()
+        self._ck(self._lib.efs_time_phases(self._h, int(steps), ms))
+        return dict(zip(PHASES, (round(v, 4) for v in ms)))
+
     def setPlaneDepth(self, xchunk):
         """Tuning (efs_set_plane_depth): x-planes per CTA of the fused kernel
         (default 32); results are bit-identical under every depth."""
@@ -527,6 +538,13 @@ class CudaBatch:
 
     def setShape(self, xchunk, ctas_per_sm=2):
         self._ck(self._lib.efs_batch_set_shape(self._h, int(xchunk), int(ctas_per_sm)))
+
+    def timePhases(self, steps=16):
+        """Diagnostics (efs_batch_time_phases): device ms per timestep of each
+        phase of a batched step (advances the members by `steps`)."""
+        ms = (C.c_float * len(PHASES))()
+        self._ck(self._lib.efs_batch_time_phases(self._h, int(steps), ms))
+        return dict(zip(PHASES, (round(v, 4) for v in ms)))
 
     def autotune(self, steps=16):
         """Pick plane depth and CTAs per SM by timing real steps (advances the

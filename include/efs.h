@@ -314,9 +314,25 @@ efs_status efs_debug_set_wait(efs_engine* e, uint64_t wait_ns, uint32_t skip_pla
  * No counterpart in the reference. */
 efs_status efs_set_plane_depth(efs_engine* e, uint32_t xchunk);
 
+/* Diagnostics: device time per timestep of each phase of the step, over
+ * `steps` (1..64) timesteps launched kernel by kernel with events between the
+ * phases (not as a graph; the engine advances as by efs_iterate and the
+ * results are the same).  ms[EFS_PHASES], mean ms per timestep:
+ *   0 steady-state accumulation and the UPML E pass (with the previous
+ *     step's NF2FF samples in the same launch when they are paired),
+ *   1 point operations before the core update (ADE, Mur pre, RLC pre),
+ *   2 fused core update, 3 E-side point operations (TFSF, PBC, Mur
+ *     post/apply, excitation, RLC, ADE apply), 4 UPML H pass and deferred H
+ *     recompute (one launch), 5 H-side point operations, 6 NF2FF samples /
+ *     accumulation and probe ring.
+ * No counterpart in the reference. */
+#define EFS_PHASES 7
+efs_status efs_time_phases(efs_engine* e, uint32_t steps, float* ms);
+
 /* Diagnostics: kernel launches one timestep enqueues with the current
  * configuration (a captured batch of n steps adds one counter update and,
- * with NF2FF configured, ceil(n/16) accumulator passes). */
+ * with NF2FF configured, ceil(n/16) accumulator passes and, when the samples
+ * ride on the next step's UPML E pass, one sample pass for its last step). */
 efs_status efs_kernels_per_step(efs_engine* e, uint32_t* out);
 
 /* --- batched form ------------------------------------------------------
@@ -348,6 +364,11 @@ efs_status efs_batch_set_shape(efs_batch* b, uint32_t xchunk, uint32_t ctas_per_
  * The timed steps advance the members (bit-identical under every shape):
  * the batch moves forward by 17*steps timesteps in all. */
 efs_status efs_batch_autotune(efs_batch* b, uint32_t steps, uint32_t* xchunk, uint32_t* ctas_per_sm, float* ms_per_step);
+/* Diagnostics: device ms per timestep of each phase of a batched step, over
+ * `steps` (1..64) timesteps launched kernel by kernel (phases as in
+ * efs_time_phases, each for all members); the batch advances as by
+ * efs_batch_iterate. */
+efs_status efs_batch_time_phases(efs_batch* b, uint32_t steps, float* ms);
 
 #ifdef __cplusplus
 }

@@ -161,3 +161,32 @@ def test_batch_rejects_unsupported_members(cuda_engine_cls):
         CudaBatch([g, g])
     g.destroy()
     odd.destroy()
+
+
+@pytest.mark.parametrize("indexed", [False, True])
+def test_phase_timing_runs_the_same_steps(cuda_engine_cls, indexed):
+    """efs_time_phases / efs_batch_time_phases advance exactly as iterate does
+    (kernel by kernel instead of a graph) and report non-negative phase times."""
+    from efs_b200.engine import PHASES, CudaBatch
+    kinds = (0, 1, 3)
+    solo = [member(cuda_engine_cls, k, indexed) for k in kinds]
+    timed = [member(cuda_engine_cls, k, indexed) for k in kinds]
+    for s, t in zip(solo, timed):
+        s.iterate(21)
+        ph = t.timePhases(21)
+        assert set(ph) == set(PHASES) and all(v >= 0 for v in ph.values()) and ph["core"] > 0
+    for k, s, t in zip(kinds, solo, timed):
+        compare(s, t, k, "timePhases")
+    b = CudaBatch(timed)
+    try:
+        ph = b.timePhases(13)
+        assert set(ph) == set(PHASES) and all(v >= 0 for v in ph.values()) and ph["core"] > 0
+        b.sync()
+    finally:
+        b.destroy()
+    for s in solo:
+        s.iterate(13)
+    for k, s, t in zip(kinds, solo, timed):
+        compare(s, t, k, "batch timePhases")
+    for e in solo + timed:
+        e.destroy()
