@@ -524,6 +524,7 @@ def run_b200(args):
     nf_passes = sum(math.ceil(m / 16) for m in chunks) if job.get("nf2ff") else 0
     launches = args.steps * (BATCH * eng.kernelsPerStep() + len(chunks) + nf_passes + 2)
     phases = eng.timePhases(32)              # per-phase device ms per timestep, launched kernel by kernel
+    tfsf_faces = [int(v) for v in eng.debugRead("tfsf_faces")]
     far = None
     if rank == 0 and world == 1 and not args.no_far_field and job.get("nf2ff"):
         far = far_field_leg(eng, job, local)
@@ -591,7 +592,7 @@ def run_b200(args):
                               "unit": "GB/s", "frac": round(step_bytes / (ms_max / steps_total / 1e3) / 1e9 / peak, 4),
                               "what": "whole timestep (all kernels) against its algorithmic bytes"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "phases_ms": phases,
+            "phases_ms": phases, "tfsf_faces_in_core": tfsf_faces,
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "batched": batched,

@@ -27,7 +27,7 @@ namespace efs {
 
 // ---- core update over all members ------------------------------------------
 struct BatchMember {            // one member at one step parity (tensor maps first: 64-byte aligned)
-    CUtensorMap tmH, tmE, tmM;
+    CUtensorMap tmH, tmE, tmM, tmD;
     FusedGrid g;
     PmlSet ps;
 };
@@ -44,7 +44,7 @@ k_fused_tma_batch(const BatchMember* __restrict__ mem, const BatchTile* __restri
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const BatchTile w = tiles[t];
         const BatchMember& M = mem[w.m];
-        if (!tma_tile<IDX, true>(S, &M.tmH, &M.tmE, &M.tmM, M.g, M.ps, w.xs, w.y0, w.z0, K)) return;
+        if (!tma_tile_body<IDX, true, true>(S, &M.tmH, &M.tmE, &M.tmM, &M.tmD, M.g, M.ps, w.xs, w.y0, w.z0, K)) return;
     }
 }
 
@@ -82,6 +82,10 @@ struct OpPoints {
 struct OpAde {
     const float* F; AdeDev a;
     __device__ void run(uint32_t blk, uint32_t, uint32_t, uint32_t) const { ade_body(F, a, blk * blockDim.x + threadIdx.x); }
+};
+struct OpTfsfFace {
+    const StepState* st; TfsfFaceDev t;
+    __device__ void run(uint32_t blk, uint32_t k, uint32_t, uint32_t) const { tfsf_face_body(st, k, t, blk * blockDim.x + threadIdx.x); }
 };
 struct OpAdeApply {
     float* F; AdeApplyDev a; uint32_t runs;
@@ -167,7 +171,7 @@ struct efs_batch {
     uint32_t ntiles[2] = {0, 0};
     SegLaunch mur_pre[2], mur_post[2], mur_apply[2], exc[2], tfsf_v[2], tfsf_c[2], ade_v[2], ade_c[2], ade_apply_v[2], ade_apply_c[2],
         ring[2], nf_sample[2], nf_flush[2],
-        deferred_i[2], deferred_d[2], pml_e_i[2], pml_e_d[2], pml_h_i[2], pml_h_d[2], advance;   // _i / _d: index / dense members
+        deferred_i[2], deferred_d[2], pml_e_i[2], pml_e_d[2], pml_h_i[2], pml_h_d[2], tfsf_face[2], advance;   // _i / _d: index / dense members
     bool any_nf = false;
     std::map<uint32_t, cudaGraphExec_t> graphs;
 
@@ -238,6 +242,7 @@ struct efs_batch {
             std::vector<std::pair<uint32_t, OpAde>> vav, vac;
             std::vector<std::pair<uint32_t, OpAdeApply>> vpv, vpc;
             std::vector<std::pair<uint32_t, OpRing>> vring;
+            std::vector<std::pair<uint32_t, OpTfsfFace>> vtf;
             std::vector<std::pair<uint32_t, OpNfSample>> vns;
             std::vector<std::pair<uint32_t, OpNfFlush>> vnf;
             std::vector<std::pair<uint32_t, OpDeferred<true>>> vdi;
@@ -258,6 +263,7 @@ struct efs_batch {
                 M.tmH = e->tensor_map(fg.H0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, bh);
                 M.tmE = e->tensor_map(fg.V0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, be);
                 M.tmM = e->indexed ? e->tensor_map(fg.mat, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, be) : M.tmE;
+                M.tmD = e->tf.n ? e->tf_map() : M.tmE;
                 M.g = fg;
                 M.g.xchunk = xchunk;
                 M.ps = ps;
@@ -294,6 +300,7 @@ struct efs_batch {
                     (side == 0 ? vpv : vpc).push_back({thr, OpAdeApply{side == 0 ? V1 : C1, e->ade_apply_dev(as), as.app_runs ? 1u : 0u}});
                 }
                 if (e->ring_on) vring.push_back({e->ring_n, OpRing{V1, C1, st, e->ring_dev()}});
+                if (e->tf_n) vtf.push_back({e->tf_n, OpTfsfFace{st, e->tf_dev()}});
                 if (e->nf_on) {
                     vns.push_back({e->nf.np, OpNfSample{V1, C1, e->nf}});
                     vnf.push_back({e->nf.np, OpNfFlush{st, e->nf}});
@@ -326,6 +333,7 @@ struct efs_batch {
             build_seg(ade_apply_v[s], vpv);
             build_seg(ade_apply_c[s], vpc);
             build_seg(ring[s], vring);
+            build_seg(tfsf_face[s], vtf);
             build_seg(nf_sample[s], vns);
             build_seg(nf_flush[s], vnf);
             build_seg(deferred_i[s], vdi);
@@ -368,6 +376,7 @@ struct efs_batch {
         launch_seg<OpAde>(ade_v[s], k);          // pre-voltage, as the single engine: ADE(volt), Mur pre
         launch_seg<OpMurPre>(mur_pre[s], k);
         launch_seg<OpAde>(ade_c[s], k);          // ADE(curr) before the core update rewrites H and the flux
+        launch_seg<OpTfsfFace>(tfsf_face[s], k); // TFSF face values the core update adds
         mark(2);
         const BatchMember* bm = members[s].as<BatchMember>();
         if (ntiles[1])

@@ -346,6 +346,7 @@ struct efs_engine {
         g.status = d_status;
         g.wait_ns = wait_ns;
         g.skip_plane = skip_plane;
+        g.tf = tf;
         return g;
     }
     // UPML set whose flux pointers are the parity-p buffers
@@ -398,6 +399,7 @@ struct efs_engine {
             upload(vflux_ptrs[p], vp);
             upload(cflux_ptrs[p], cp);
         }
+        plan_tfsf_faces();
         build_deferred();
         if (mur_on) {
             std::vector<ReadLoc> rn(mur_n), rs(mur_n);
@@ -481,6 +483,27 @@ struct efs_engine {
     // H cells whose curl reads an E value rewritten by a sparse post-update
     // operation (TFSF, PBC, Mur apply, excitation, series RLC) are updated
     // after those operations by k_deferred_h.  Targets are device indices.
+    // TFSF face corrections applied in the core update (TfsfFace): up to two z
+    // planes holding many single-entry Ex/Ey targets (the box's z faces).
+    // Their entries leave the point pass, and the deferred set: the H cells
+    // next to them see the corrected E inside the core update.
+    std::vector<efs_tfsf_point> h_tfsf_v;      // the caller's voltage-side TFSF points
+    TfsfFace tf{0, {0, 0}};
+    uint32_t tf_n = 0, tf_ly = 0;
+    DevBuf tf_face, tf_dst, tf_delay, tf_frac, tf_amp;
+    void plan_tfsf_faces();
+    TfsfFaceDev tf_dev() const {
+        return TfsfFaceDev{tf_n, tf_dst.as<uint32_t>(), tf_delay.as<uint32_t>(), tf_frac.as<float>(), tf_amp.as<float>(),
+                           tfsf_signal.as<float>(), tfsf_len, tfsf_period, tf_face.as<float>()};
+    }
+    // tensor map of the face array: dims y (pitch tf_ly), x, component, face; box TF_DY x 1 x 2 x faces
+    CUtensorMap tf_map() const {
+        const cuuint64_t dims[4] = {Ny, Nx, 2, tf.n};
+        const cuuint64_t strides[3] = {(cuuint64_t)tf_ly * 4, (cuuint64_t)Nx * tf_ly * 4, (cuuint64_t)2 * Nx * tf_ly * 4};
+        const uint32_t box[4] = {(uint32_t)TF_DY, 1, 2, tf.n};
+        return encode_map(tf_face.p, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, dims, strides, box);
+    }
+
     void build_deferred() {
         defer_n = 0;
         std::vector<uint32_t> mod;   // modified E entries as n*Nd + device cell
@@ -600,6 +623,7 @@ struct efs_engine {
         // ADE(curr) reads H and the current flux, which the E side never
         // touches: it runs before the fused kernel overwrites the flux.
         if (ade_c.live()) k_ade<<<blocks(ade_c.n, ADE_BLOCK), ADE_T, 0, stream>>>(C, ade_dev(ade_c, cfl));
+        if (tf_n) k_tfsf_face<<<blocks(tf_n, T), T, 0, stream>>>(st, k, tf_dev());   // TFSF face values of this step
         mark(2);
         launch_fused_tma(p);
         mark(3);
@@ -705,6 +729,13 @@ struct efs_engine {
     // rows (the grid's Nz x Ny x Nx cells over the padded layout), boxes of
     // one tile plus halos (efs_tma.cuh)
     CUtensorMap tensor_map(const void* base, CUtensorMapDataType dt, uint32_t rank, const uint32_t box[4]) const {
+        const cuuint64_t dims[4] = {Nz, Ny, Nx, 3};
+        const cuuint64_t strides[3] = {(cuuint64_t)Pz * 4, (cuuint64_t)Ny * Pz * 4, (cuuint64_t)Nd * 4};
+        return encode_map(base, dt, rank, dims, strides, box);
+    }
+    // dims: innermost first; strides: bytes of dimensions 1.. (multiples of 16)
+    static CUtensorMap encode_map(const void* base, CUtensorMapDataType dt, uint32_t rank, const cuuint64_t* dims,
+                                  const cuuint64_t* strides, const uint32_t* box) {
         static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
         if (!encode) {
             void* fn = nullptr;
@@ -713,9 +744,8 @@ struct efs_engine {
             if (q != cudaDriverEntryPointSuccess || !fn) fail(EFS_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
             encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
         }
-        const cuuint64_t dims[4] = {Nz, Ny, Nx, 3};
-        const cuuint64_t strides[3] = {(cuuint64_t)Pz * 4, (cuuint64_t)Ny * Pz * 4, (cuuint64_t)Nd * 4};
-        const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+        cuuint32_t bx[4] = {1, 1, 1, 1};
+        for (uint32_t i = 0; i < rank; ++i) bx[i] = box[i];
         const cuuint32_t es[4] = {1, 1, 1, 1};
         CUtensorMap m;
         const CUresult r = encode(&m, dt, rank, const_cast<void*>(base), dims, strides, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -724,15 +754,15 @@ struct efs_engine {
         return m;
     }
     template <bool IDX, bool PML>
-    void launch_fused_tma_k(dim3 g, const CUtensorMap& tH, const CUtensorMap& tE, const CUtensorMap& tM, const FusedGrid& fg,
-                            const PmlSet& ps) {
+    void launch_fused_tma_k(dim3 g, const CUtensorMap& tH, const CUtensorMap& tE, const CUtensorMap& tM, const CUtensorMap& tD,
+                            const FusedGrid& fg, const PmlSet& ps) {
         static bool attr_set = false;   // per instantiation; the attribute is per kernel, all devices alike
         if (!attr_set) {
             ck(cudaFuncSetAttribute(k_fused_tma<IDX, PML>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT_SMEM_BYTES),
                "smem attr");
             attr_set = true;
         }
-        k_fused_tma<IDX, PML><<<g, TT_THREADS, TT_SMEM_BYTES, stream>>>(tH, tE, tM, fg, ps);
+        k_fused_tma<IDX, PML><<<g, TT_THREADS, TT_SMEM_BYTES, stream>>>(tH, tE, tM, tD, fg, ps);
     }
     void launch_fused_tma(int p) {
         const FusedGrid fg = fused_grid(p);
@@ -741,10 +771,11 @@ struct efs_engine {
         const CUtensorMap tH = tensor_map(fg.H0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, bh);
         const CUtensorMap tE = tensor_map(fg.V0, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, be);
         const CUtensorMap tM = indexed ? tensor_map(fg.mat, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, be) : tE;
+        const CUtensorMap tD = tf.n ? tf_map() : tE;   // unused without TFSF faces
         dim3 g(blocks(Nz, TT_Z), blocks(Ny, TT_Y), blocks(Nx, xchunk));
         const bool hp = !pml.empty();
-        if (indexed) { if (hp) launch_fused_tma_k<true, true>(g, tH, tE, tM, fg, ps); else launch_fused_tma_k<true, false>(g, tH, tE, tM, fg, ps); }
-        else { if (hp) launch_fused_tma_k<false, true>(g, tH, tE, tM, fg, ps); else launch_fused_tma_k<false, false>(g, tH, tE, tM, fg, ps); }
+        if (indexed) { if (hp) launch_fused_tma_k<true, true>(g, tH, tE, tM, tD, fg, ps); else launch_fused_tma_k<true, false>(g, tH, tE, tM, tD, fg, ps); }
+        else { if (hp) launch_fused_tma_k<false, true>(g, tH, tE, tM, tD, fg, ps); else launch_fused_tma_k<false, false>(g, tH, tE, tM, tD, fg, ps); }
     }
     // UPML cells are updated by k_pml_e / k_pml_h around the fused kernel
     bool pml_split() const { return !pml.empty(); }
@@ -901,6 +932,9 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     e->gd_n = 0;
     e->Nx = dims[0]; e->Ny = dims[1]; e->Nz = dims[2]; e->N = N; e->Pz = Pz; e->Nd = Nd;
     e->h_exc_targets.clear(); e->h_tfsf_v_targets.clear(); e->h_mur_apply.clear(); e->h_rlc_series.clear();
+    e->h_tfsf_v.clear();
+    e->tf = TfsfFace{0, {0, 0}};
+    e->tf_n = 0;
     e->defer_n = 0;
     // plane depth (x-planes per CTA) of the fused kernel; results do not depend on it
     e->cur = 0;
@@ -1205,6 +1239,71 @@ static void build_points(efs_engine* e, efs_engine::PointSet& ps, const efs_tfsf
     ps.groups = (uint32_t)ut.size();
 }
 
+// TFSF faces of the core update: up to two z planes, each holding at least a
+// 16th of the voltage-side entries as single-entry Ex/Ey targets (the box's z
+// faces); their entries move to the face array, every other entry stays in
+// the point pass (in the caller's order per target).
+void efs_engine::plan_tfsf_faces() {
+    tf = TfsfFace{0, {0, 0}};
+    tf_n = 0;
+    tf_face.reset(); tf_dst.reset(); tf_delay.reset(); tf_frac.reset(); tf_amp.reset();
+    if (!tfsf_on) return;
+    const size_t nv = h_tfsf_v.size();
+    std::vector<uint32_t> tg(nv);
+    for (size_t i = 0; i < nv; ++i) tg[i] = dev_index(h_tfsf_v[i].field_idx);
+    std::vector<uint32_t> sorted = tg;
+    std::sort(sorted.begin(), sorted.end());
+    auto single = [&](uint32_t t) {
+        auto r = std::equal_range(sorted.begin(), sorted.end(), t);
+        return r.second - r.first == 1;
+    };
+    std::vector<uint8_t> cand(nv, 0);
+    std::vector<size_t> per_z(Nz, 0);
+    for (size_t i = 0; i < nv; ++i) {
+        const uint32_t n = tg[i] / (uint32_t)Nd;
+        if (n > 1 || !single(tg[i])) continue;
+        cand[i] = 1;
+        ++per_z[(tg[i] % Nd) % Pz];
+    }
+    std::vector<uint32_t> faces;
+    if (Ny >= (uint32_t)TF_DY)
+        for (int k = 0; k < 2; ++k) {
+            uint32_t best = Nz;
+            for (uint32_t z = 0; z < Nz; ++z)
+                if (per_z[z] * 16 >= nv && per_z[z] > 0 && (best == Nz || per_z[z] > per_z[best]) &&
+                    (faces.empty() || z != faces[0]))
+                    best = z;
+            if (best < Nz) faces.push_back(best);
+        }
+    const uint32_t ly = (Ny + 3) & ~3u;
+    std::vector<efs_tfsf_point> rest;
+    std::vector<uint32_t> dst, delay;
+    std::vector<float> frac, amp;
+    for (size_t i = 0; i < nv; ++i) {
+        int f = -1;
+        const uint32_t z = (tg[i] % Nd) % Pz;
+        for (size_t q = 0; q < faces.size(); ++q) if (cand[i] && z == faces[q]) f = (int)q;
+        if (f < 0) { rest.push_back(h_tfsf_v[i]); continue; }
+        const uint32_t n = tg[i] / (uint32_t)Nd, c = tg[i] % (uint32_t)Nd;
+        const uint32_t x = c / (Ny * Pz), y = (c / Pz) % Ny;
+        dst.push_back(((uint32_t)(f * 2 + n) * Nx + x) * ly + y);
+        delay.push_back(h_tfsf_v[i].delay_int); frac.push_back(h_tfsf_v[i].delay_frac); amp.push_back(h_tfsf_v[i].amp);
+    }
+    build_points(this, tfsf_v, rest.data(), (uint32_t)rest.size());
+    h_tfsf_v_targets.clear();
+    for (auto& p : rest) h_tfsf_v_targets.push_back(dev_index(p.field_idx));
+    if (faces.empty()) return;
+    const size_t nface = faces.size() * 2 * (size_t)Nx * ly;
+    alloc(tf_face, nface * 4, false);
+    k_fill<<<(unsigned)std::min<size_t>(blocks(nface, 256), 4096), 256, 0, stream>>>(tf_face.as<float>(), nface, -0.0f);
+    ck(cudaGetLastError(), "face fill");
+    upload(tf_dst, dst); upload(tf_delay, delay); upload(tf_frac, frac); upload(tf_amp, amp);
+    tf.n = (uint32_t)faces.size();
+    for (size_t q = 0; q < faces.size(); ++q) tf.z[q] = faces[q];
+    tf_n = (uint32_t)dst.size();
+    tf_ly = ly;
+}
+
 efs_status efs_configure_tfsf(efs_engine* e, const float* signal, uint32_t L, uint32_t period, const efs_tfsf_point* vp,
                               uint32_t nv, const efs_tfsf_point* cp, uint32_t nc) {
     return guard(e, [&] {
@@ -1212,6 +1311,7 @@ efs_status efs_configure_tfsf(efs_engine* e, const float* signal, uint32_t L, ui
         if (!signal || L == 0) fail(EFS_ERR_INVALID, "TFSF signal must be non-empty");
         if ((nv && !vp) || (nc && !cp)) fail(EFS_ERR_INVALID, "TFSF point arrays must be non-null");
         build_points(e, e->tfsf_v, vp, nv);
+        e->h_tfsf_v.assign(vp, vp + nv);
         e->h_tfsf_v_targets.clear();
         for (uint32_t i = 0; i < nv; ++i) e->h_tfsf_v_targets.push_back(e->dev_index(vp[i].field_idx));
         build_points(e, e->tfsf_c, cp, nc);
@@ -1830,6 +1930,15 @@ efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* 
         std::string s(name);
         const DevBuf* b = nullptr;
         size_t n = 0;
+        if (s == "tfsf_faces") {   // planned TFSF z faces of the core update (count, then each face's z)
+            e->build_plan();
+            if (count) *count = 1 + e->tf.n;
+            if (!out) return;
+            if (cap < 1 + e->tf.n) fail(EFS_ERR_INVALID, "output buffer too small");
+            out[0] = (float)e->tf.n;
+            for (uint32_t f = 0; f < e->tf.n; ++f) out[1 + f] = (float)e->tf.z[f];
+            return;
+        }
         if ((s == "pml_volt_flux" || s == "pml_curr_flux") && arg < e->pml.size()) {
             const int p = e->cur;
             auto& R = *e->pml[arg];

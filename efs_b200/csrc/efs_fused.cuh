@@ -37,7 +37,13 @@ struct FusedGrid {
     uint32_t* status;                   // device status word (bit 0: a bounded wait ran out)
     uint64_t wait_ns;                   // limit of every bounded mbarrier wait (about 1 s)
     uint32_t skip_plane;                // diagnostics: loads of this x-plane are never issued (~0u: none)
+    TfsfFace tf;                        // TFSF z faces corrected in the core update (tf.n == 0: none)
 };
+
+// Face of z plane z among the TFSF faces the core update corrects, or -1.
+__device__ __forceinline__ int tf_face(const TfsfFace& tf, uint32_t z) {
+    return tf.n > 0 && z == tf.z[0] ? 0 : (tf.n > 1 && z == tf.z[1]) ? 1 : -1;
+}
 
 // UPML chain with separate old/new flux buffers; up to PML_MAX_OVERLAP regions per cell.
 template <bool VOLT>

@@ -445,6 +445,48 @@ __global__ void k_advance(StepState* st, uint32_t n) { st->numTS += n; }
 // ---------------------------------------------------------------------------
 constexpr int NF_MAX_FREQ = 16;
 constexpr uint32_t NF_K = 16;       // steps of surface samples buffered between accumulator passes
+// TFSF E corrections of up to two z planes (the box's z faces), applied by the
+// fused update as it computes E instead of by the point pass after it: per
+// step k_tfsf_face writes, for every TFSF target on those planes that has a
+// single entry (Ex or Ey), the value the point pass would add (amplitude x
+// interpolated incident signal) into a dense array [face][Ex, Ey][x][y] (row
+// pitch ly, a multiple of 4 floats).  Every other cell holds -0.0f, which
+// adds as the identity (x + -0 == x for every x, signed zeros included), as
+// does an entry outside its signal window.
+struct TfsfFace {
+    uint32_t n;                     // faces (0: none)
+    uint32_t z[2];
+};
+constexpr int TF_DY = 12;           // staged rows of a face array per plane (>= tile rows + halo, 16-byte inner box)
+struct TfsfFaceDev {
+    uint32_t n;                     // entries
+    const uint32_t* dst;            // index into the face array
+    const uint32_t* delay; const float* frac; const float* amp;
+    const float* signal; uint32_t len, period;
+    float* face;                    // [face][2][Nx][ly]
+};
+__device__ __forceinline__ void tfsf_face_body(const StepState* st, uint32_t k, const TfsfFaceDev& t, uint32_t i) {
+    if (i >= t.n) return;
+    const int64_t ts = (int64_t)st->numTS + k;
+    float v = -0.0f;                // the identity when the entry adds nothing this step
+    int64_t d = ts - (int64_t)t.delay[i];
+    if (d >= 0) {
+        if (t.period > 0) d %= (int64_t)t.period;
+        if (d < (int64_t)t.len - 1) {   // point_sources_body<1>'s value, the same operations
+            const float delta = t.frac[i];
+            const float sig = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, delta), t.signal[d]), __fmul_rn(delta, t.signal[d + 1]));
+            v = __fmul_rn(t.amp[i], sig);
+        }
+    }
+    t.face[t.dst[i]] = v;
+}
+__global__ void k_tfsf_face(const StepState* st, uint32_t k, const TfsfFaceDev t) {
+    tfsf_face_body(st, k, t, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_fill(float* p, size_t n, float v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
 struct Nf2ffDev {
     uint32_t np, nf, maxTS, window;
     uint32_t Nx, Ny, Nz, Pz;        // Pz: z pitch of the device layout

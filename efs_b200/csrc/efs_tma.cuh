@@ -60,6 +60,7 @@ struct TmaStage {
     alignas(128) float H[3][TT_HY][TT_HZ];
     alignas(128) float E[3][TT_EY][TT_EZ];
     alignas(128) uint32_t M[TT_EY][TT_EZ];
+    alignas(128) float D[2][2][TF_DY];   // TFSF face corrections of the plane: [face][Ex, Ey][row]
 };
 struct TmaSmem {
     TmaStage st[TT_S];
@@ -108,17 +109,20 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// Issue the loads of plane x into stage s (one thread).
+// Issue the loads of plane x into stage s (one thread); dbytes > 0: also the
+// plane's TFSF face corrections (rows y0 .. y0+TF_DY-1 of every face).
 template <bool IDX>
 __device__ __forceinline__ void tt_issue(TmaSmem& S, int s, const CUtensorMap* tmH, const CUtensorMap* tmE,
-                                         const CUtensorMap* tmM, int x, int y0, int z0) {
+                                         const CUtensorMap* tmM, const CUtensorMap* tmD, uint32_t dbytes, int x, int y0,
+                                         int z0) {
     const uint32_t bar = smem_u32(&S.full[s]);
-    const uint32_t bytes = TT_H_BYTES + TT_E_BYTES + (IDX ? TT_M_BYTES : 0u);
+    const uint32_t bytes = TT_H_BYTES + TT_E_BYTES + (IDX ? TT_M_BYTES : 0u) + dbytes;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of the stage before the refill
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
     tma_load_4d(&S.st[s].H[0][0][0], tmH, z0 - 4, y0 - 1, x, 0, bar);
     tma_load_4d(&S.st[s].E[0][0][0], tmE, z0, y0, x, 0, bar);
     if (IDX) tma_load_3d(&S.st[s].M[0][0], tmM, z0, y0, x, bar);
+    if (dbytes) tma_load_4d(&S.st[s].D[0][0][0], tmD, y0, x, 0, 0, bar);
 }
 
 // The CTA's shared working area: 128-byte aligned, addressed from the shared
@@ -143,10 +147,12 @@ __device__ __forceinline__ void tt_init(TmaSmem& S) {
 // consumed before this tile (it selects the stage, the mbarrier phase and the
 // E_new buffer, so one CTA can run tiles back to back); every load the tile
 // issues is consumed before it returns.  Returns false after a wait ran out.
-template <bool IDX, bool PML>
-__device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, const CUtensorMap* tmE, const CUtensorMap* tmM,
-                                         const FusedGrid& g, const PmlSet& ps, uint32_t xs, uint32_t y0, uint32_t z0,
-                                         uint32_t& K) {
+// TF: the tile may meet a TFSF face corrected here (tested per tile; the single
+// engine runs tiles that meet none through the instantiation without that code).
+template <bool IDX, bool PML, bool TF>
+__device__ __forceinline__ bool tma_tile_body(TmaSmem& S, const CUtensorMap* tmH, const CUtensorMap* tmE, const CUtensorMap* tmM,
+                                              const CUtensorMap* tmD, const FusedGrid& g, const PmlSet& ps, uint32_t xs,
+                                              uint32_t y0, uint32_t z0, uint32_t& K) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t xe = min(xs + g.xchunk, g.Nx);
     const uint32_t xl = xe < g.Nx ? xe : g.Nx - 1;           // last plane whose E this CTA computes
@@ -186,12 +192,21 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
             for (int q = 0; q < 3; ++q) yzm[q] = axis_mask(ps, cand, 1, sy[q]) & axis_mask(ps, cand, 2, sz[q]);
     }
 
+    bool tf_tile = false;
+    if (TF)
+        for (uint32_t f = 0; f < g.tf.n; ++f) tf_tile |= g.tf.z[f] >= z0 && g.tf.z[f] <= z0 + TT_Z;
+    const uint32_t dbytes = tf_tile ? g.tf.n * 2u * TF_DY * 4u : 0u;
+    int tfq[3] = {-1, -1, -1};
+    if (tf_tile)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) tfq[q] = sin[q] ? tf_face(g.tf, sz[q]) : -1;
+
     // ---- first planes into the pipeline
     int issued = 0;                                          // planes issued (thread 0's count)
     if (threadIdx.x == 0)
         for (; issued < TT_S && issued < nk; ++issued)
             if (xs + issued != g.skip_plane)
-                tt_issue<IDX>(S, (int)((K + issued) % TT_S), tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);
+                tt_issue<IDX>(S, (int)((K + issued) % TT_S), tmH, tmE, tmM, tmD, dbytes, (int)(xs + issued), (int)y0, (int)z0);
 
     // H_old(xs-1) of the E cells (y, z components); at xs = 0 the x-1 neighbour is plane 0 itself
     float hp[3][3];
@@ -258,6 +273,11 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
                 en[q][0] = upml ? eo[q][0] : upd(eo[q][0], kk[q][0], kk[q][3], cx);
                 en[q][1] = upml ? eo[q][1] : upd(eo[q][1], kk[q][1], kk[q][4], cy);
                 en[q][2] = upml ? eo[q][2] : upd(eo[q][2], kk[q][2], kk[q][5], cz);
+                if (tf_tile && tfq[q] >= 0) {               // the TFSF point pass's add, here
+                    const float* D = &S.st[s].D[tfq[q]][0][0];
+                    en[q][0] = __fadd_rn(en[q][0], D[sr[q]]);
+                    en[q][1] = __fadd_rn(en[q][1], D[TF_DY + sr[q]]);
+                }
             }
             float* V1 = g.V1 + px;
 #pragma unroll
@@ -276,8 +296,8 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
         timed_out = __syncthreads_or(!ok) != 0;
         if (timed_out) break;
         if (threadIdx.x == 0 && issued < nk) {
-            if (xs + issued != g.skip_plane)
-                tt_issue<IDX>(S, s, tmH, tmE, tmM, (int)(xs + issued), (int)y0, (int)z0);   // stage of plane k+TT_S
+            if (xs + issued != g.skip_plane)   // stage of plane k+TT_S
+                tt_issue<IDX>(S, s, tmH, tmE, tmM, tmD, dbytes, (int)(xs + issued), (int)y0, (int)z0);
             ++issued;
         }
         // ---- H_new(x-1) of the owned cells
@@ -343,17 +363,28 @@ __device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, con
     K += nk;
     return true;
 }
+// A TFSF face corrected in the core update meets the tile's columns (halo column included).
+template <bool IDX, bool PML>
+__device__ __forceinline__ bool tma_tile(TmaSmem& S, const CUtensorMap* tmH, const CUtensorMap* tmE, const CUtensorMap* tmM,
+                                         const CUtensorMap* tmD, const FusedGrid& g, const PmlSet& ps, uint32_t xs,
+                                         uint32_t y0, uint32_t z0, uint32_t& K) {
+    bool tf = false;
+    for (uint32_t f = 0; f < g.tf.n; ++f) tf |= g.tf.z[f] >= z0 && g.tf.z[f] <= z0 + TT_Z;
+    return tf ? tma_tile_body<IDX, PML, true>(S, tmH, tmE, tmM, tmD, g, ps, xs, y0, z0, K)
+              : tma_tile_body<IDX, PML, false>(S, tmH, tmE, tmM, tmD, g, ps, xs, y0, z0, K);
+}
 
 template <bool IDX, bool PML>
 __global__ void __launch_bounds__(TT_THREADS, 2)
 k_fused_tma(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmE,
-            const __grid_constant__ CUtensorMap tmM, const FusedGrid g, const PmlSet ps) {
+            const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmD, const FusedGrid g,
+            const PmlSet ps) {
     const uint32_t xs = blockIdx.z * g.xchunk;
     if (xs >= g.Nx) return;                                  // uniform per CTA
     TmaSmem& S = tt_smem();
     tt_init(S);
     uint32_t K = 0;
-    (void)tma_tile<IDX, PML>(S, &tmH, &tmE, &tmM, g, ps, xs, blockIdx.y * TT_Y, blockIdx.x * TT_Z, K);
+    (void)tma_tile<IDX, PML>(S, &tmH, &tmE, &tmM, &tmD, g, ps, xs, blockIdx.y * TT_Y, blockIdx.x * TT_Z, K);
 }
 
 // ---------------------------------------------------------------------------

@@ -285,8 +285,9 @@ efs_status efs_device_bytes(const efs_engine* e, size_t* out);
  * Names: "pml_volt_flux", "pml_curr_flux" (arg = region), "mur_saved",
  * "ade_volt", "ade_volt_lor", "ade_curr", "ade_curr_lor" (all orders and
  * directions concatenated in configuration order), "rlc_vdn", "rlc_jn",
- * "rlc_vil" (caller's element order), "pbc_imag".  out == NULL queries the
- * count.  Mirrors the reference tests' direct reads of engine state
+ * "rlc_vil" (caller's element order), "pbc_imag", "tfsf_faces" (the planned
+ * TFSF z faces whose E corrections the fused update applies: count, then
+ * each face's z).  out == NULL queries the count.  Mirrors the reference tests' direct reads of engine state
  * (tests/test_webgpu.mjs, e.g. :1215, :1946, :2224).  No counterpart in the
  * engine class itself. */
 efs_status efs_debug_read(efs_engine* e, const char* name, uint32_t arg, float* out, size_t cap, size_t* count);

@@ -325,6 +325,39 @@ def test_tfsf_on_tile_seams_bitexact(cuda_engine_cls):
         assert_bitexact(g.debugRead("pml_curr_flux", k), o.read("pml_curr_flux", k), "cflux %d" % k)
 
 
+@pytest.mark.parametrize("indexed", [False, True])
+def test_tfsf_faces_in_core_bitexact(cuda_engine_cls, indexed):
+    """Dense Ex/Ey TFSF targets on two z planes (63: last owned column of a
+    64-wide tile, 64: its halo column and the next tile's first column) are
+    added inside the fused update from a per-step face array; repeated targets
+    on those planes, targets of other components and scattered targets stay in
+    the point pass, some inside a UPML region."""
+    N = (13, 20, 136)
+    g, o = both(cuda_engine_cls, N, rand_coeffs(N, 50) if not indexed else free_space(*N), indexed)
+    regs = [pml_region((0, 12, 0), (13, 8, 136), 51)]
+    for e in (g, o):
+        e.configurePML(regs)
+    r = np.random.default_rng(52)
+    pt = lambda n, x, y, z: dict(field_idx=idx(n, x, y, z, *N), delay_int=int(r.integers(0, 8)),
+                                 delay_frac=float(r.random()), amp=float(r.standard_normal()))
+    vp = [pt(n, x, y, z) for z in (63, 64) for x in range(N[0]) for y in range(N[1]) for n in (0, 1)]
+    vp += [pt(int(r.integers(0, 3)), int(r.integers(0, N[0])), int(r.integers(0, N[1])), int(r.integers(0, N[2])))
+           for _ in range(120)]
+    vp += [dict(vp[i]) for i in range(0, len(vp), 37)]     # repeated targets: back to the point pass, in order
+    cp = [pt(int(r.integers(0, 3)), int(r.integers(0, N[0])), int(r.integers(0, N[1])), int(r.integers(0, N[2])))
+          for _ in range(80)]
+    cfg = dict(signal=np.sin(np.arange(40) * 0.35).astype(np.float32), period=0, voltagePoints=vp, currentPoints=cp)
+    for e in (g, o):
+        e.configureTFSF(cfg)
+    assert sorted(g.debugRead("tfsf_faces")[1:]) == [63, 64]
+    seed_fields(g, o, N, 53)
+    for n in (1, 5, 44):                                  # past the signal's end too (identity adds)
+        g.iterate(n)
+        o.iterate(n)
+        compare_fields(g, o, "tfsf faces +%d" % n)
+    assert_bitexact(g.debugRead("pml_curr_flux", 0), o.read("pml_curr_flux", 0), "cflux")
+
+
 @pytest.mark.parametrize("apply", [False, True])
 def test_ade_in_and_out_of_pml_bitexact(cuda_engine_cls, apply):
     """Two orders on the same cells (with the apply step: entries grouped per
