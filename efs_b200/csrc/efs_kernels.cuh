@@ -755,6 +755,20 @@ __global__ void k_ff_prep(const float* __restrict__ meta, const float* __restric
     r.m = make_float4(s * E[2 * cb], s * E[2 * cb + 1], -s * E[2 * ca], -s * E[2 * ca + 1]);
     rec[i] = r;
 }
+// One (angle, point) pair: the record's tangential currents times e^{j 2 pi phase}
+// added into a (N_a, N_b, L_a, L_b as re, im).
+__device__ __forceinline__ void ff_pair(const FfRecord& r, float ux, float uy, float uz, float (&a)[8]) {
+    float ph = r.pos.x * ux;
+    ph = fmaf(r.pos.y, uy, ph);
+    ph = fmaf(r.pos.z, uz, ph);
+    ph -= rintf(ph);                                       // turns in [-1/2, 1/2]
+    float sn, cs;
+    __sincosf(6.2831853071795864f * ph, &sn, &cs);
+    a[0] = fmaf(r.j.x, cs, fmaf(-r.j.y, sn, a[0])); a[1] = fmaf(r.j.y, cs, fmaf(r.j.x, sn, a[1]));
+    a[2] = fmaf(r.j.z, cs, fmaf(-r.j.w, sn, a[2])); a[3] = fmaf(r.j.w, cs, fmaf(r.j.z, sn, a[3]));
+    a[4] = fmaf(r.m.x, cs, fmaf(-r.m.y, sn, a[4])); a[5] = fmaf(r.m.y, cs, fmaf(r.m.x, sn, a[5]));
+    a[6] = fmaf(r.m.z, cs, fmaf(-r.m.w, sn, a[6])); a[7] = fmaf(r.m.w, cs, fmaf(r.m.z, sn, a[7]));
+}
 // Records [p0, p1) of normal axis ND for this thread's angle (direction u).
 template <int ND>
 __device__ __forceinline__ void ff_segment(const FarFieldDev& d, FfRecord* tile, uint32_t p0, uint32_t p1, float ux, float uy,
@@ -766,20 +780,20 @@ __device__ __forceinline__ void ff_segment(const FarFieldDev& d, FfRecord* tile,
         for (uint32_t j = threadIdx.x; j < nt; j += FF_THREADS) tile[j] = d.rec[t0 + j];
         __syncthreads();
         if (!live) continue;
+        // four points per iteration into two sets of sums: their phases and
+        // sines / cosines are independent, so several are in flight per thread
         float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // N_a, N_b, L_a, L_b (re, im)
-        for (uint32_t j = q; j < nt; j += FF_PL) {
-            const FfRecord& r = tile[j];
-            float ph = r.pos.x * ux;
-            ph = fmaf(r.pos.y, uy, ph);
-            ph = fmaf(r.pos.z, uz, ph);
-            ph -= rintf(ph);                                   // turns in [-1/2, 1/2]
-            float sn, cs;
-            __sincosf(6.2831853071795864f * ph, &sn, &cs);
-            s[0] = fmaf(r.j.x, cs, fmaf(-r.j.y, sn, s[0])); s[1] = fmaf(r.j.y, cs, fmaf(r.j.x, sn, s[1]));
-            s[2] = fmaf(r.j.z, cs, fmaf(-r.j.w, sn, s[2])); s[3] = fmaf(r.j.w, cs, fmaf(r.j.z, sn, s[3]));
-            s[4] = fmaf(r.m.x, cs, fmaf(-r.m.y, sn, s[4])); s[5] = fmaf(r.m.y, cs, fmaf(r.m.x, sn, s[5]));
-            s[6] = fmaf(r.m.z, cs, fmaf(-r.m.w, sn, s[6])); s[7] = fmaf(r.m.w, cs, fmaf(r.m.z, sn, s[7]));
+        float t[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        uint32_t j = q;
+        for (; j + 3 * FF_PL < nt; j += 4 * FF_PL) {
+            ff_pair(tile[j], ux, uy, uz, s);
+            ff_pair(tile[j + FF_PL], ux, uy, uz, t);
+            ff_pair(tile[j + 2 * FF_PL], ux, uy, uz, s);
+            ff_pair(tile[j + 3 * FF_PL], ux, uy, uz, t);
         }
+        for (; j < nt; j += FF_PL) ff_pair(tile[j], ux, uy, uz, s);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s[i] += t[i];
         acc[2 * CA] += s[0]; acc[2 * CA + 1] += s[1];
         acc[2 * CB] += s[2]; acc[2 * CB + 1] += s[3];
         acc[6 + 2 * CA] += s[4]; acc[6 + 2 * CA + 1] += s[5];
