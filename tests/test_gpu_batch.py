@@ -62,6 +62,18 @@ def member(cls, kind, indexed):
             job = dict(job, coefficients=dict(vv=vv, vi=vi, ii=ii, iv=iv))
         from efs_b200.workloads import configure
         configure(g, job)
+    elif kind == 4:                       # dense TFSF z faces (added inside the core update) + scattered entries
+        N = (10, 14, 70)
+        g.init(N, coeffs(N, 9, indexed))
+        pt = lambda n, x, y, z: dict(field_idx=idx(n, x, y, z, *N), delay_int=int(r.integers(0, 6)),
+                                     delay_frac=float(r.random()), amp=float(r.standard_normal()))
+        vp = [pt(n, x, y, z) for z in (30, 64) for x in range(N[0]) for y in range(N[1]) for n in (0, 1)]
+        vp += [pt(int(r.integers(0, 3)), int(r.integers(0, N[0])), int(r.integers(0, N[1])), int(r.integers(0, N[2])))
+               for _ in range(40)]
+        cp = [pt(int(r.integers(0, 3)), int(r.integers(0, N[0])), int(r.integers(0, N[1])), int(r.integers(0, N[2])))
+              for _ in range(30)]
+        g.configureTFSF(dict(signal=np.sin(np.arange(30) * 0.4).astype(np.float32), period=0, voltagePoints=vp,
+                             currentPoints=cp))
     else:                                 # small grid, excitation only; Nz = 7 (padded rows)
         N = (9, 11, 7)
         g.init(N, coeffs(N, 7, indexed))
@@ -101,9 +113,10 @@ def compare(a, b, kind, what):
 @pytest.mark.parametrize("indexed", [True, False])
 def test_batch_members_match_solo_engines(cuda_engine_cls, indexed):
     from efs_b200.engine import CudaBatch
-    kinds = (0, 1, 2, 3)
+    kinds = (0, 1, 2, 3, 4)
     batched = [member(cuda_engine_cls, k, indexed) for k in kinds]
     solo = [member(cuda_engine_cls, k, indexed) for k in kinds]
+    assert sorted(batched[4].debugRead("tfsf_faces")[1:]) == [30, 64]   # faces applied in the batched core
     b = CudaBatch(batched)
     try:
         for n, shape in ((1, None), (17, (4, 1)), (70, (8, 2)), (5, (3, 2))):
