@@ -23,18 +23,19 @@ from collections import deque
 import numpy as np
 
 from . import workloads
-from .engine import CudaBatch, CudaEngine
+from .engine import CudaBatch, CudaEngine, EfsError
 
 
 class Request:
     __slots__ = ("rid", "job", "steps", "arrival", "admitted", "done", "engine", "remaining", "slices", "result", "cells",
-                 "saved", "evictions")
+                 "saved", "evictions", "retry_below")
 
     def __init__(self, rid, job, steps, arrival):
         self.rid, self.job, self.steps, self.arrival = rid, job, int(steps), arrival
         self.admitted = self.done = None
         self.saved = None                          # host copy of an evicted solve's state (efs_get_state)
         self.evictions = 0
+        self.retry_below = None                    # device bytes in use when its admission last failed
         self.engine = None
         self.remaining = int(steps)
         self.slices = None
@@ -82,6 +83,7 @@ class Server:
         self.waiting = deque()
         self.active = []
         self.finished = []
+        self.failed = []                           # requests whose engine could not be set up alone
         self.used = 0
         self.batch = None
         self.next_id = 0
@@ -107,13 +109,34 @@ class Server:
             need = estimate_bytes(r.job)
             if self.used + need > self.budget and self.active:
                 break                                           # wait for memory to free up
+            if r.retry_below is not None and self.used >= r.retry_below and self.active:
+                break                                           # failed beside the same residents: wait
             self.waiting.popleft()
             e = CudaEngine(device=self.device)
-            e.initGPU()
-            r.slices = workloads.configure(e, r.job)
-            if r.saved is not None:                             # an evicted solve resumes where it stopped
-                e.setState(r.saved)
+            try:
+                if not e.initGPU():
+                    raise EfsError(3, "no usable CUDA device %r" % (self.device,))
+                r.slices = workloads.configure(e, r.job)
+                if r.saved is not None:                         # an evicted solve resumes where it stopped
+                    e.setState(r.saved)
+            except (EfsError, MemoryError) as exc:
+                # The engine's allocations (cudaMalloc inside configure, or
+                # the state upload) failed: free what it holds.  Beside other
+                # resident solves the request waits at the head of the queue
+                # until they have released memory; alone on the device it can
+                # never run, and is reported as failed.
+                e.destroy()
+                if self.active:
+                    r.retry_below = self.used
+                    self.waiting.appendleft(r)
+                    break
+                r.result = {"error": str(exc)}
+                r.done = self.now()
                 r.saved = None
+                self.failed.append(r)
+                continue
+            r.saved = None
+            r.retry_below = None
             r.engine = e
             if r.admitted is None:
                 r.admitted = self.now()
@@ -302,7 +325,7 @@ def main():
     print(json.dumps({"arrivals": len(stream), "rate": args.rate, "duration_s": args.duration, "wall_s": round(wall, 2),
                       "template_prep_s": round(prep, 1), "latency": latency_stats(done),
                       "solves_per_s": round(len(done) / wall, 3), "mcells_s": round(srv.cell_steps / wall / 1e6, 1),
-                      "unserved": len(stream) - len(done), "members": args.members, "budget_gb": args.budget_gb}))
+                      "unserved": len(stream) - len(done) - len(srv.failed), "failed": len(srv.failed), "members": args.members, "budget_gb": args.budget_gb}))
 
 
 if __name__ == "__main__":

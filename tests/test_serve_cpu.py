@@ -13,9 +13,12 @@ from efs_b200 import serve
 
 class FakeEngine:
     energy_log = []                             # (grid side, reduction used) per retirement
+    made = []                                   # every engine constructed
+
     def __init__(self, device=0):
         self.steps, self.bytes, self.destroyed = 0, 0, False
         self.numLines = [4, 4, 4]
+        FakeEngine.made.append(self)
 
     def initGPU(self):
         return True
@@ -68,11 +71,19 @@ def fake(monkeypatch):
     monkeypatch.setattr(serve, "CudaBatch", FakeBatch)
 
     def configure(engine, job):
+        live = [e for e in FakeEngine.made if not e.destroyed and e is not engine]
+        fail = job.get("fail")                  # "always", or "beside": only while other solves are resident
+        if fail == "always" or (fail == "beside" and live):
+            fake.configure_failures += 1
+            raise serve.EfsError(4, "cudaMalloc failed (fake)")
         engine.bytes = job["bytes"]
         engine.numLines = list(job.get("grid", (4, 4, 4)))
         return None
     monkeypatch.setattr(serve.workloads, "configure", configure)
-    return FakeBatch
+    FakeEngine.made = []
+    fake = FakeBatch
+    fake.configure_failures = 0
+    return fake
 
 
 def job(side, nbytes):
@@ -187,6 +198,40 @@ def test_eviction_respects_the_limit_and_ratio(fake):
     drain(s)
     assert s.evicted == 1                         # at most once per solve
     assert {r.rid: r for r in s.finished}[a].result["energy"] == 3000.0
+
+
+def test_a_request_that_cannot_allocate_alone_fails_cleanly(fake):
+    s = serve.Server(hbm_budget=1e15, max_members=4, chunk=100)
+    ok1 = s.submit(job(16, 1000), 300, arrival=0.0)
+    bad = s.submit(dict(job(24, 1000), fail="always"), 200, arrival=0.0)
+    ok2 = s.submit(job(32, 1000), 150, arrival=0.0)
+    drain(s)
+    assert sorted(r.rid for r in s.finished) == [ok1, ok2]
+    assert [r.rid for r in s.failed] == [bad]
+    r = s.failed[0]
+    assert "EFS_ERR_OOM" in r.result["error"] and r.engine is None and r.done is not None
+    assert all(e.destroyed for e in FakeEngine.made)           # the failed engine was freed too
+    assert s.used == 0 and not s.waiting and not s.active
+    # it failed beside residents first (waits), then alone (fails): two attempts
+    assert fake.configure_failures == 2
+
+
+def test_a_request_that_fails_beside_residents_waits_for_them(fake):
+    s = serve.Server(hbm_budget=1e15, max_members=4, chunk=100)
+    a = s.submit(job(16, 1000), 1000, arrival=0.0)
+    s.round()
+    late = s.submit(dict(job(24, 1000), fail="beside"), 250, arrival=0.0)
+    b = s.submit(job(16, 1000), 100, arrival=0.0)      # behind it in arrival order
+    drain(s)
+    assert not s.failed
+    by = {r.rid: r for r in s.finished}
+    assert set(by) == {a, late, b}
+    assert by[late].result["energy"] == 250.0
+    assert by[late].admitted >= by[a].done                      # admitted once the resident solve left
+    assert by[b].admitted >= by[late].admitted                  # arrival order kept behind it
+    # one failed attempt: no retry while the same solves stay resident
+    assert fake.configure_failures == 1
+    assert s.used == 0 and all(e.destroyed for e in FakeEngine.made)
 
 
 def test_request_stream_and_latency_stats():
