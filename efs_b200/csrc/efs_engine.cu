@@ -38,10 +38,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -138,10 +140,13 @@ struct efs_engine {
 
     // Caller index (n*N + x*Ny*Nz + y*Nz + z, the reference's NIJK order) ->
     // device index (n*Nd + (x*Ny + y)*Pz + z).
+    // 32-bit arithmetic holds: 3 * Nd < 2^32 (alloc_fields) and N <= Nd.
     uint32_t dev_index(uint32_t f) const {
-        const uint64_t n = f / N, cell = f - n * N, nyz = (uint64_t)Ny * Nz;
-        const uint64_t x = cell / nyz, r = cell - x * nyz, y = r / Nz, z = r - y * Nz;
-        return (uint32_t)(n * Nd + (x * Ny + y) * Pz + z);
+        if (Pz == Nz) return f;                              // no padding: the layouts coincide
+        const uint32_t N32 = (uint32_t)N, nyz = Ny * Nz;
+        const uint32_t n = f / N32, cell = f - n * N32;
+        const uint32_t x = cell / nyz, r = cell - x * nyz, y = r / Nz, z = r - y * Nz;
+        return n * (uint32_t)Nd + (x * Ny + y) * Pz + z;
     }
     size_t dev_cell(uint64_t x, uint64_t y, uint64_t z) const { return (size_t)((x * Ny + y) * Pz + z); }
     // Host array of `comps` components in the caller's layout -> device
@@ -312,19 +317,27 @@ struct efs_engine {
     }
 
     void need_init() const { if (!inited) fail(EFS_ERR_STATE, "engine not initialised: call efs_init first"); }
-    // Stable LSD radix sort of (key, value) pairs by key (8-bit digits; digits
-    // above the largest key are skipped).
+    // Stable LSD radix sort of (key, value) pairs by key (11-bit digits; digits
+    // above the largest key are skipped; input already in key order is left
+    // as it is).
     static void radix_sort_pairs(std::vector<uint32_t>& key, std::vector<uint32_t>& val) {
         const size_t n = key.size();
         uint32_t kmax = 0;
-        for (uint32_t k : key) kmax = std::max(kmax, k);
-        std::vector<uint32_t> k2(n), v2(n);
-        for (int shift = 0; shift < 32 && (shift == 0 || (kmax >> shift) != 0); shift += 8) {
-            size_t cnt[257] = {0};
-            for (size_t i = 0; i < n; ++i) ++cnt[((key[i] >> shift) & 255u) + 1];
-            for (int d = 0; d < 256; ++d) cnt[d + 1] += cnt[d];
+        bool sorted = true;
+        for (size_t i = 0; i < n; ++i) {
+            kmax = std::max(kmax, key[i]);
+            sorted = sorted && (i == 0 || key[i - 1] <= key[i]);
+        }
+        if (sorted) return;
+        constexpr int B = 11;
+        constexpr uint32_t M = (1u << B) - 1;
+        std::vector<uint32_t> k2(n), v2(n), cnt(M + 2);
+        for (int shift = 0; shift < 32 && (shift == 0 || (kmax >> shift) != 0); shift += B) {
+            std::fill(cnt.begin(), cnt.end(), 0u);
+            for (size_t i = 0; i < n; ++i) ++cnt[((key[i] >> shift) & M) + 1];
+            for (uint32_t d = 0; d <= M; ++d) cnt[d + 1] += cnt[d];
             for (size_t i = 0; i < n; ++i) {
-                const size_t o = cnt[(key[i] >> shift) & 255u]++;
+                const uint32_t o = cnt[(key[i] >> shift) & M]++;
                 k2[o] = key[i]; v2[o] = val[i];
             }
             key.swap(k2); val.swap(v2);
@@ -370,12 +383,11 @@ struct efs_engine {
     // pre-update: the flux slot of the last region containing the cell, else
     // the field itself.
     ReadLoc redirect(uint32_t field_idx) const {
-        uint32_t n = field_idx / (uint32_t)Nd;
-        size_t cell = field_idx - (size_t)n * Nd;
-        uint32_t x = (uint32_t)(cell / ((size_t)Ny * Pz));
-        uint32_t y = (uint32_t)((cell / Pz) % Ny);
-        uint32_t z = (uint32_t)(cell % Pz);
         ReadLoc l{0, field_idx};
+        if (pml.empty()) return l;
+        const uint32_t n = field_idx / (uint32_t)Nd;
+        const uint32_t cell = field_idx - n * (uint32_t)Nd;
+        const uint32_t row = cell / Pz, z = cell - row * Pz, x = row / Ny, y = row - x * Ny;
         for (size_t r = 0; r < pml.size(); ++r) {
             const Region& R = *pml[r];
             if ((x - R.s[0]) < R.n[0] && (y - R.s[1]) < R.n[1] && (z - R.s[2]) < R.n[2]) {
@@ -528,31 +540,33 @@ struct efs_engine {
                     }
             }
         if (mod.empty()) return;
-        const size_t NyPz = (size_t)Ny * Pz;
+        // 32-bit cell arithmetic: Nd < 2^32 / 3
+        const uint32_t NyPz = Ny * Pz, Nd32 = (uint32_t)Nd;
         std::vector<uint32_t> bits((Nd + 31) / 32, 0);
-        auto mark = [&](int64_t x, int64_t y, int64_t z) {
-            if (x < 0 || y < 0 || z < 0) return;
-            const size_t c = dev_cell(x, y, z);
-            bits[c >> 5] |= 1u << (c & 31);
-        };
+        auto mark = [&](uint32_t c) { bits[c >> 5] |= 1u << (c & 31); };
         for (uint32_t f : mod) {
-            const uint32_t n = f / (uint32_t)Nd;
-            const size_t cell = f - (size_t)n * Nd;
-            const int64_t x = cell / NyPz, y = (cell / Pz) % Ny, z = cell % Pz;
+            const uint32_t n = f / Nd32, cell = f - n * Nd32;
+            const uint32_t row = cell / Pz, z = cell - row * Pz, x = row / Ny, y = row - x * Ny;
             // E_n(m) appears in the curls of H at m, m - e_a, m - e_b (a, b != n)
-            mark(x, y, z);
-            if (n != 0) mark(x - 1, y, z);
-            if (n != 1) mark(x, y - 1, z);
-            if (n != 2) mark(x, y, z - 1);
+            mark(cell);
+            if (n != 0 && x > 0) mark(cell - NyPz);
+            if (n != 1 && y > 0) mark(cell - Pz);
+            if (n != 2 && z > 0) mark(cell - 1);
         }
-        // UPML cells are left to k_pml_h, which runs after the E-side operations
+        // UPML cells are left to k_pml_h, which runs after the E-side
+        // operations: clear each region row's z run [c, c + n_z)
         for (auto& R : pml)
             for (uint32_t x = R->s[0]; x < R->s[0] + R->n[0]; ++x)
-                for (uint32_t y = R->s[1]; y < R->s[1] + R->n[1]; ++y)
-                    for (uint32_t z = R->s[2]; z < R->s[2] + R->n[2]; ++z) {
-                        const size_t c = dev_cell(x, y, z);
-                        bits[c >> 5] &= ~(1u << (c & 31));
+                for (uint32_t y = R->s[1]; y < R->s[1] + R->n[1]; ++y) {
+                    uint32_t c = (x * Ny + y) * Pz + R->s[2];
+                    const uint32_t end = c + R->n[2];
+                    while (c < end) {
+                        const uint32_t w = c >> 5, b0 = c & 31, b1 = std::min<uint32_t>(32, b0 + (end - c));
+                        const uint32_t m = (b1 == 32 ? ~0u : ((1u << b1) - 1)) & ~((1u << b0) - 1);
+                        bits[w] &= ~m;
+                        c += b1 - b0;
                     }
+                }
         std::vector<uint32_t> cells;
         for (size_t w = 0; w < bits.size(); ++w)
             for (uint32_t b = bits[w]; b; b &= b - 1) cells.push_back((uint32_t)(w * 32 + __builtin_ctz(b)));
@@ -1051,11 +1065,24 @@ efs_status efs_init_indexed(efs_engine* e, const uint32_t dims[3], const uint32_
     return guard(e, [&] {
         if (!mat || !table || ntable == 0) fail(EFS_ERR_INVALID, "mat/table must be non-null and ntable > 0");
         alloc_fields(e, dims);
-        for (size_t c = 0; c < e->N; ++c)
-            if (mat[c] >= ntable) fail(EFS_ERR_INVALID, "material index out of range");
+        // indices are checked on the device after the upload (pad cells hold 0)
+        e->upload_padded(e->mat, mat, 1);
+        {
+            DevBuf mx;
+            e->alloc(mx, 4);
+            k_max_u32<<<std::min<uint32_t>(blocks(e->Nd, 256), 148 * 8), 256, 0, e->stream>>>(e->mat.as<uint32_t>(), e->Nd,
+                                                                                               mx.as<uint32_t>());
+            ck(cudaGetLastError(), "material index check");
+            uint32_t hmax = 0;
+            ck(cudaMemcpyAsync(&hmax, mx.p, 4, cudaMemcpyDeviceToHost, e->stream), "material index check");
+            e->sync("material index check");
+            if (hmax >= ntable) {
+                e->mat.reset();
+                fail(EFS_ERR_INVALID, "material index out of range");
+            }
+        }
         e->indexed = true;
         e->ntable = ntable;
-        e->upload_padded(e->mat, mat, 1);
         e->upload(e->table, table, (size_t)ntable * 12);
         e->sync_state_to_device();
         e->inited = true;
@@ -1093,7 +1120,13 @@ efs_status efs_configure_excitation(efs_engine* e, const float* signal, uint32_t
 // region's cells as a row table and a 16-bit row index per cell.  A UPML's
 // coefficients follow its grading profiles, so a slab has a few thousand
 // distinct tuples at most; a region with more keeps only the dense arrays.
-static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_region& in) {
+struct PmlCompact {
+    std::vector<uint16_t> idx;
+    std::vector<float> tab;
+    bool ok = false;
+};
+static PmlCompact compact_pml(const efs_engine::Region& R, const efs_pml_region& in) {
+    PmlCompact out;
     const size_t nc = R.total / 3;
     const float* src[6] = {in.vv, in.vvfo, in.vvfn, in.ii, in.iifo, in.iifn};
     typedef std::array<uint32_t, 18> Key;
@@ -1105,8 +1138,9 @@ static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_regi
         }
     };
     std::unordered_map<Key, uint32_t, KeyHash> ids;
-    std::vector<uint16_t> idx(nc);
-    std::vector<float> tab;
+    std::vector<uint16_t>& idx = out.idx;
+    std::vector<float>& tab = out.tab;
+    idx.resize(nc);
     // Lookups skip the map when the tuple equals the previous cell's (grading
     // along x or y: constant along a z row) or the previous row's at the same
     // z (grading along z: a z-slab row repeats its tuples).
@@ -1126,7 +1160,7 @@ static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_regi
         } else {
             auto it = ids.find(key);
             if (it == ids.end()) {
-                if (ids.size() >= 65535) { R.cidx.reset(); R.ctab.reset(); return; }
+                if (ids.size() >= 65535) return PmlCompact{};
                 it = ids.emplace(key, (uint32_t)ids.size()).first;
                 for (int a = 0; a < 6; ++a) {
                     for (int n = 0; n < 3; ++n) { float f; memcpy(&f, &key[a * 3 + n], 4); tab.push_back(f); }
@@ -1140,8 +1174,8 @@ static void compact_pml(efs_engine* e, efs_engine::Region& R, const efs_pml_regi
         zid[z] = last_id;
         idx[c] = (uint16_t)last_id;
     }
-    e->upload(R.cidx, idx);
-    e->upload(R.ctab, tab);
+    out.ok = true;
+    return out;
 }
 
 efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region* regions) {
@@ -1161,12 +1195,37 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
             }
             if (!in.vv || !in.vvfo || !in.vvfn || !in.ii || !in.iifo || !in.iifn) fail(EFS_ERR_INVALID, "PML region array missing");
             R->total = 3 * (size_t)R->n[0] * R->n[1] * R->n[2];
-            e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
-            e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
-            compact_pml(e, *R, in);
-            e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
-            e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4);
             out.push_back(std::move(R));
+        }
+        // the regions' coefficient tables are built on host threads (one per
+        // region) while this thread uploads the dense arrays
+        std::vector<PmlCompact> comp(count);
+        std::vector<std::exception_ptr> errs(count);
+        std::vector<std::thread> workers;
+        auto join = [&] { for (auto& t : workers) if (t.joinable()) t.join(); };
+        try {
+            for (uint32_t r = 0; r < count; ++r)
+                workers.emplace_back([&, r] {
+                    try { comp[r] = compact_pml(*out[r], regions[r]); } catch (...) { errs[r] = std::current_exception(); }
+                });
+            for (uint32_t r = 0; r < count; ++r) {
+                const efs_pml_region& in = regions[r];
+                efs_engine::Region* R = out[r].get();
+                e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
+                e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
+                e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
+                e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4);
+            }
+        } catch (...) {
+            join();
+            throw;
+        }
+        join();
+        for (uint32_t r = 0; r < count; ++r) {
+            if (errs[r]) std::rethrow_exception(errs[r]);
+            if (!comp[r].ok) continue;
+            e->upload(out[r]->cidx, comp[r].idx);
+            e->upload(out[r]->ctab, comp[r].tab);
         }
         // the per-cell UPML chain keeps at most PML_MAX_OVERLAP regions in registers:
         // test every corner formed by region bounds (the overlap count is maximal at one)
@@ -1251,19 +1310,25 @@ void efs_engine::plan_tfsf_faces() {
     const size_t nv = h_tfsf_v.size();
     std::vector<uint32_t> tg(nv);
     for (size_t i = 0; i < nv; ++i) tg[i] = dev_index(h_tfsf_v[i].field_idx);
-    std::vector<uint32_t> sorted = tg;
-    std::sort(sorted.begin(), sorted.end());
-    auto single = [&](uint32_t t) {
-        auto r = std::equal_range(sorted.begin(), sorted.end(), t);
-        return r.second - r.first == 1;
-    };
+    // entries in target order (stable: the caller's order per target); the
+    // entries whose target no other entry shares are runs of length 1
+    std::vector<uint32_t> key(tg), perm(nv);
+    for (size_t i = 0; i < nv; ++i) perm[i] = (uint32_t)i;
+    radix_sort_pairs(key, perm);
+    std::vector<uint8_t> single(nv, 0);
+    for (size_t i = 0; i < nv;) {
+        size_t j = i + 1;
+        while (j < nv && key[j] == key[i]) ++j;
+        if (j == i + 1) single[perm[i]] = 1;
+        i = j;
+    }
     std::vector<uint8_t> cand(nv, 0);
     std::vector<size_t> per_z(Nz, 0);
     for (size_t i = 0; i < nv; ++i) {
         const uint32_t n = tg[i] / (uint32_t)Nd;
-        if (n > 1 || !single(tg[i])) continue;
+        if (n > 1 || !single[i]) continue;
         cand[i] = 1;
-        ++per_z[(tg[i] % Nd) % Pz];
+        ++per_z[(tg[i] % (uint32_t)Nd) % Pz];
     }
     std::vector<uint32_t> faces;
     if (Ny >= (uint32_t)TF_DY)
@@ -1276,22 +1341,40 @@ void efs_engine::plan_tfsf_faces() {
             if (best < Nz) faces.push_back(best);
         }
     const uint32_t ly = (Ny + 3) & ~3u;
-    std::vector<efs_tfsf_point> rest;
+    std::vector<uint8_t> on_face(nv, 0);
     std::vector<uint32_t> dst, delay;
     std::vector<float> frac, amp;
     for (size_t i = 0; i < nv; ++i) {
         int f = -1;
-        const uint32_t z = (tg[i] % Nd) % Pz;
+        const uint32_t z = (tg[i] % (uint32_t)Nd) % Pz;
         for (size_t q = 0; q < faces.size(); ++q) if (cand[i] && z == faces[q]) f = (int)q;
-        if (f < 0) { rest.push_back(h_tfsf_v[i]); continue; }
+        if (f < 0) continue;
+        on_face[i] = 1;
         const uint32_t n = tg[i] / (uint32_t)Nd, c = tg[i] % (uint32_t)Nd;
         const uint32_t x = c / (Ny * Pz), y = (c / Pz) % Ny;
         dst.push_back(((uint32_t)(f * 2 + n) * Nx + x) * ly + y);
         delay.push_back(h_tfsf_v[i].delay_int); frac.push_back(h_tfsf_v[i].delay_frac); amp.push_back(h_tfsf_v[i].amp);
     }
-    build_points(this, tfsf_v, rest.data(), (uint32_t)rest.size());
-    h_tfsf_v_targets.clear();
-    for (auto& p : rest) h_tfsf_v_targets.push_back(dev_index(p.field_idx));
+    // the point pass keeps the other entries, grouped by target in target
+    // order (what build_points makes of them: face entries are whole groups)
+    {
+        std::vector<uint32_t> ut, off(1, 0), d;
+        std::vector<float> a, fr;
+        for (size_t k = 0; k < nv; ++k) {
+            const uint32_t i = perm[k];
+            if (on_face[i]) continue;
+            if (ut.empty() || key[k] != ut.back()) {
+                if (!ut.empty()) off.push_back((uint32_t)d.size());
+                ut.push_back(key[k]);
+            }
+            d.push_back(h_tfsf_v[i].delay_int); a.push_back(h_tfsf_v[i].amp); fr.push_back(h_tfsf_v[i].delay_frac);
+        }
+        if (!d.empty()) off.push_back((uint32_t)d.size());
+        upload(tfsf_v.target, ut); upload(tfsf_v.off, off); upload(tfsf_v.delay, d); upload(tfsf_v.amp, a);
+        upload(tfsf_v.frac, fr);
+        tfsf_v.groups = (uint32_t)ut.size();
+        h_tfsf_v_targets = ut;
+    }
     if (faces.empty()) return;
     const size_t nface = faces.size() * 2 * (size_t)Nx * ly;
     alloc(tf_face, nface * 4, false);
@@ -1310,11 +1393,14 @@ efs_status efs_configure_tfsf(efs_engine* e, const float* signal, uint32_t L, ui
         e->need_init();
         if (!signal || L == 0) fail(EFS_ERR_INVALID, "TFSF signal must be non-empty");
         if ((nv && !vp) || (nc && !cp)) fail(EFS_ERR_INVALID, "TFSF point arrays must be non-null");
-        build_points(e, e->tfsf_v, vp, nv);
+        std::vector<uint32_t> vt(nv);
+        for (uint32_t i = 0; i < nv; ++i) vt[i] = vp[i].field_idx;
+        e->check_idx3(vt.data(), nv, "TFSF field_idx");
+        build_points(e, e->tfsf_c, cp, nc);
+        // the voltage side's point set and targets are built by the plan
+        // (plan_tfsf_faces), once the core update's z faces are chosen
         e->h_tfsf_v.assign(vp, vp + nv);
         e->h_tfsf_v_targets.clear();
-        for (uint32_t i = 0; i < nv; ++i) e->h_tfsf_v_targets.push_back(e->dev_index(vp[i].field_idx));
-        build_points(e, e->tfsf_c, cp, nc);
         e->upload(e->tfsf_signal, signal, L);
         e->tfsf_len = L; e->tfsf_period = period;
         e->tfsf_on = true;

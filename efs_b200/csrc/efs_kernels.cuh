@@ -486,6 +486,14 @@ __global__ void k_tfsf_face(const StepState* st, uint32_t k, const TfsfFaceDev t
 __global__ void k_fill(float* p, size_t n, float v) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
+// Largest element of a uint32 array, folded into *out (atomicMax; *out starts at 0).
+__global__ void k_max_u32(const uint32_t* __restrict__ a, size_t n, uint32_t* out) {
+    uint32_t m = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = max(m, __ldg(a + i));
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
 
 struct Nf2ffDev {
     uint32_t np, nf, maxTS, window;
