@@ -86,6 +86,63 @@ void ck(cudaError_t err, const char* what) {
 
 inline uint32_t blocks(size_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
+// Host threads for a loop over n items of configure-time work (1 below 64 K items).
+inline unsigned host_threads(size_t n) {
+    if (n < (1u << 16)) return 1;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return (unsigned)std::min<size_t>({(size_t)std::min(hw, 16u), n >> 15});
+}
+
+// f(t, lo, hi) on T contiguous chunks of [0, n), chunk t on its own thread
+// (chunk 0 on the caller's).  f must not throw.
+template <class F>
+void parallel_chunks(size_t n, unsigned T, F&& f) {
+    if (T <= 1) { f(0u, (size_t)0, n); return; }
+    std::vector<std::thread> th;
+    th.reserve(T - 1);
+    for (unsigned t = 1; t < T; ++t) th.emplace_back([&, t] { f(t, n * t / T, n * (t + 1) / T); });
+    f(0u, (size_t)0, n / T);
+    for (auto& x : th) x.join();
+}
+
+// An engine's pinned host words: the status word its kernels set through a
+// mapped pointer (bit 0: a bounded device wait ran out) and two slots of
+// energy results.  They are 32-byte slots of mapped, portable pinned pages
+// that live as long as the process and are handed out again after an
+// engine's destruction, so creating and destroying engines neither allocates
+// nor frees pinned memory (cudaFreeHost of a mapped page has taken up to
+// 0.6 s on B200 hosts).
+struct HostSlot {
+    uint32_t status;
+    uint32_t pad0;
+    double energy[2];
+    uint64_t pad1;
+};
+static_assert(sizeof(HostSlot) == 32, "host slot layout");
+std::mutex g_slot_mu;
+std::vector<HostSlot*> g_free_slots;
+
+HostSlot* host_slot_get() {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    if (g_free_slots.empty()) {
+        constexpr size_t PAGE = 4096;
+        void* p = nullptr;
+        ck(cudaHostAlloc(&p, PAGE, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc");
+        HostSlot* s = static_cast<HostSlot*>(p);
+        for (size_t i = PAGE / sizeof(HostSlot); i-- > 0;) g_free_slots.push_back(s + i);
+    }
+    HostSlot* s = g_free_slots.back();
+    g_free_slots.pop_back();
+    memset(s, 0, sizeof(*s));
+    return s;
+}
+
+void host_slot_put(HostSlot* s) {
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    g_free_slots.push_back(s);
+}
+
 }  // namespace
 
 struct efs_engine {
@@ -126,6 +183,7 @@ struct efs_engine {
         size_t total;
         DevBuf vv, vvfo, vvfn, ii, iifo, iifn, vflux, cflux, vflux_b, cflux_b;
         DevBuf cidx, ctab;      // compact coefficients (empty when the region has too many distinct tuples)
+                                // vv..iifn stay empty when the compact table serves every cell (no overlap)
         float* vf(int p) const { return (p && vflux_b.p) ? vflux_b.as<float>() : vflux.as<float>(); }
         float* cf(int p) const { return (p && cflux_b.p) ? cflux_b.as<float>() : cflux.as<float>(); }
     };
@@ -263,6 +321,7 @@ struct efs_engine {
 
     // energy (lagged, double-buffered like computeEnergy :2974-3021)
     DevBuf en_partial, en_result;
+    HostSlot* slot = nullptr;        // pinned host words of this engine (status, energy)
     double* en_host = nullptr;       // pinned, 2 slots
     // device status word in mapped pinned host memory: bit 0 = a bounded device wait ran out
     uint32_t* h_status = nullptr;
@@ -279,8 +338,7 @@ struct efs_engine {
     ~efs_engine() {
         drop_graphs();
         for (auto& ev : en_event) if (ev) cudaEventDestroy(ev);
-        if (en_host) cudaFreeHost(en_host);
-        if (h_status) cudaFreeHost(h_status);
+        host_slot_put(slot);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -319,7 +377,9 @@ struct efs_engine {
     void need_init() const { if (!inited) fail(EFS_ERR_STATE, "engine not initialised: call efs_init first"); }
     // Stable LSD radix sort of (key, value) pairs by key (11-bit digits; digits
     // above the largest key are skipped; input already in key order is left
-    // as it is).
+    // as it is).  Each pass runs on T host threads over contiguous chunks:
+    // per-chunk digit counts, offsets in (digit, chunk) order, then each chunk
+    // scatters its items in order, which keeps the sort stable.
     static void radix_sort_pairs(std::vector<uint32_t>& key, std::vector<uint32_t>& val) {
         const size_t n = key.size();
         uint32_t kmax = 0;
@@ -330,16 +390,30 @@ struct efs_engine {
         }
         if (sorted) return;
         constexpr int B = 11;
-        constexpr uint32_t M = (1u << B) - 1;
-        std::vector<uint32_t> k2(n), v2(n), cnt(M + 2);
+        constexpr uint32_t D = 1u << B, M = D - 1;
+        const unsigned T = host_threads(n);
+        std::vector<uint32_t> k2(n), v2(n);
+        std::vector<size_t> cnt((size_t)T * D);
         for (int shift = 0; shift < 32 && (shift == 0 || (kmax >> shift) != 0); shift += B) {
-            std::fill(cnt.begin(), cnt.end(), 0u);
-            for (size_t i = 0; i < n; ++i) ++cnt[((key[i] >> shift) & M) + 1];
-            for (uint32_t d = 0; d <= M; ++d) cnt[d + 1] += cnt[d];
-            for (size_t i = 0; i < n; ++i) {
-                const uint32_t o = cnt[(key[i] >> shift) & M]++;
-                k2[o] = key[i]; v2[o] = val[i];
-            }
+            std::fill(cnt.begin(), cnt.end(), (size_t)0);
+            parallel_chunks(n, T, [&](unsigned t, size_t lo, size_t hi) {
+                size_t* c = cnt.data() + (size_t)t * D;
+                for (size_t i = lo; i < hi; ++i) ++c[(key[i] >> shift) & M];
+            });
+            size_t run = 0;
+            for (uint32_t d = 0; d < D; ++d)
+                for (unsigned t = 0; t < T; ++t) {
+                    const size_t c = cnt[(size_t)t * D + d];
+                    cnt[(size_t)t * D + d] = run;
+                    run += c;
+                }
+            parallel_chunks(n, T, [&](unsigned t, size_t lo, size_t hi) {
+                size_t* o = cnt.data() + (size_t)t * D;
+                for (size_t i = lo; i < hi; ++i) {
+                    const size_t j = o[(key[i] >> shift) & M]++;
+                    k2[j] = key[i]; v2[j] = val[i];
+                }
+            });
             key.swap(k2); val.swap(v2);
         }
     }
@@ -415,7 +489,9 @@ struct efs_engine {
         build_deferred();
         if (mur_on) {
             std::vector<ReadLoc> rn(mur_n), rs(mur_n);
-            for (uint32_t i = 0; i < mur_n; ++i) { rn[i] = redirect(h_mur_normal[i]); rs[i] = redirect(h_mur_shifted[i]); }
+            parallel_chunks(mur_n, host_threads(mur_n), [&](unsigned, size_t lo, size_t hi) {
+                for (size_t i = lo; i < hi; ++i) { rn[i] = redirect(h_mur_normal[i]); rs[i] = redirect(h_mur_shifted[i]); }
+            });
             upload(mur_pre_normal, rn);
             upload(mur_pre_shifted, rs);
         }
@@ -543,16 +619,18 @@ struct efs_engine {
         // 32-bit cell arithmetic: Nd < 2^32 / 3
         const uint32_t NyPz = Ny * Pz, Nd32 = (uint32_t)Nd;
         std::vector<uint32_t> bits((Nd + 31) / 32, 0);
-        auto mark = [&](uint32_t c) { bits[c >> 5] |= 1u << (c & 31); };
-        for (uint32_t f : mod) {
-            const uint32_t n = f / Nd32, cell = f - n * Nd32;
-            const uint32_t row = cell / Pz, z = cell - row * Pz, x = row / Ny, y = row - x * Ny;
-            // E_n(m) appears in the curls of H at m, m - e_a, m - e_b (a, b != n)
-            mark(cell);
-            if (n != 0 && x > 0) mark(cell - NyPz);
-            if (n != 1 && y > 0) mark(cell - Pz);
-            if (n != 2 && z > 0) mark(cell - 1);
-        }
+        auto mark = [&](uint32_t c) { __atomic_fetch_or(&bits[c >> 5], 1u << (c & 31), __ATOMIC_RELAXED); };
+        parallel_chunks(mod.size(), host_threads(mod.size()), [&](unsigned, size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i) {
+                const uint32_t f = mod[i], n = f / Nd32, cell = f - n * Nd32;
+                const uint32_t row = cell / Pz, z = cell - row * Pz, x = row / Ny, y = row - x * Ny;
+                // E_n(m) appears in the curls of H at m, m - e_a, m - e_b (a, b != n)
+                mark(cell);
+                if (n != 0 && x > 0) mark(cell - NyPz);
+                if (n != 1 && y > 0) mark(cell - Pz);
+                if (n != 2 && z > 0) mark(cell - 1);
+            }
+        });
         // UPML cells are left to k_pml_h, which runs after the E-side
         // operations: clear each region row's z run [c, c + n_z)
         for (auto& R : pml)
@@ -567,9 +645,23 @@ struct efs_engine {
                         c += b1 - b0;
                     }
                 }
-        std::vector<uint32_t> cells;
-        for (size_t w = 0; w < bits.size(); ++w)
-            for (uint32_t b = bits[w]; b; b &= b - 1) cells.push_back((uint32_t)(w * 32 + __builtin_ctz(b)));
+        // marked cells in ascending order: per-chunk counts, then each chunk
+        // writes its cells at its offset
+        const size_t W = bits.size();
+        const unsigned T = host_threads(W);
+        std::vector<size_t> at(T + 1, 0);
+        parallel_chunks(W, T, [&](unsigned t, size_t lo, size_t hi) {
+            size_t c = 0;
+            for (size_t w = lo; w < hi; ++w) c += (size_t)__builtin_popcount(bits[w]);
+            at[t + 1] = c;
+        });
+        for (unsigned t = 0; t < T; ++t) at[t + 1] += at[t];
+        std::vector<uint32_t> cells(at[T]);
+        parallel_chunks(W, T, [&](unsigned t, size_t lo, size_t hi) {
+            size_t o = at[t];
+            for (size_t w = lo; w < hi; ++w)
+                for (uint32_t b = bits[w]; b; b &= b - 1) cells[o++] = (uint32_t)(w * 32 + __builtin_ctz(b));
+        });
         upload(defer_cells, cells);
         defer_n = (uint32_t)cells.size();
     }
@@ -992,9 +1084,9 @@ efs_status efs_create(efs_engine** out, int device) {
     try {
         ck(cudaSetDevice(device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        ck(cudaMallocHost(&e->en_host, 2 * sizeof(double)), "cudaMallocHost");
-        ck(cudaHostAlloc(&e->h_status, sizeof(uint32_t), cudaHostAllocMapped), "cudaHostAlloc");
-        *e->h_status = 0;
+        e->slot = host_slot_get();
+        e->en_host = e->slot->energy;
+        e->h_status = &e->slot->status;
         ck(cudaHostGetDevicePointer(&e->d_status, e->h_status, 0), "cudaHostGetDevicePointer");
         for (auto& ev : e->en_event) ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
     } catch (const EfsError& ex) {
@@ -1197,8 +1289,26 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
             R->total = 3 * (size_t)R->n[0] * R->n[1] * R->n[2];
             out.push_back(std::move(R));
         }
+        // A region's dense coefficient arrays are read only for cells that
+        // another region also contains (the multi-region chain) and when its
+        // compact table cannot be built: regions that overlap no other upload
+        // them only in the second case.
+        std::vector<uint8_t> overlaps(count, 0);
+        for (uint32_t a = 0; a < count; ++a)
+            for (uint32_t b = a + 1; b < count; ++b) {
+                bool meet = true;
+                for (int d = 0; d < 3; ++d)
+                    meet = meet && out[a]->s[d] < out[b]->s[d] + out[b]->n[d] && out[b]->s[d] < out[a]->s[d] + out[a]->n[d];
+                if (meet) overlaps[a] = overlaps[b] = 1;
+            }
+        auto upload_dense = [&](uint32_t r) {
+            const efs_pml_region& in = regions[r];
+            efs_engine::Region* R = out[r].get();
+            e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
+            e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
+        };
         // the regions' coefficient tables are built on host threads (one per
-        // region) while this thread uploads the dense arrays
+        // region) while this thread uploads what it can already
         std::vector<PmlCompact> comp(count);
         std::vector<std::exception_ptr> errs(count);
         std::vector<std::thread> workers;
@@ -1209,10 +1319,8 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
                     try { comp[r] = compact_pml(*out[r], regions[r]); } catch (...) { errs[r] = std::current_exception(); }
                 });
             for (uint32_t r = 0; r < count; ++r) {
-                const efs_pml_region& in = regions[r];
                 efs_engine::Region* R = out[r].get();
-                e->upload(R->vv, in.vv, R->total); e->upload(R->vvfo, in.vvfo, R->total); e->upload(R->vvfn, in.vvfn, R->total);
-                e->upload(R->ii, in.ii, R->total); e->upload(R->iifo, in.iifo, R->total); e->upload(R->iifn, in.iifn, R->total);
+                if (overlaps[r]) upload_dense(r);
                 e->alloc(R->vflux, R->total * 4); e->alloc(R->cflux, R->total * 4);
                 e->alloc(R->vflux_b, R->total * 4); e->alloc(R->cflux_b, R->total * 4);
             }
@@ -1223,7 +1331,10 @@ efs_status efs_configure_pml(efs_engine* e, uint32_t count, const efs_pml_region
         join();
         for (uint32_t r = 0; r < count; ++r) {
             if (errs[r]) std::rethrow_exception(errs[r]);
-            if (!comp[r].ok) continue;
+            if (!comp[r].ok) {
+                if (!overlaps[r]) upload_dense(r);
+                continue;
+            }
             e->upload(out[r]->cidx, comp[r].idx);
             e->upload(out[r]->ctab, comp[r].tab);
         }

@@ -367,8 +367,8 @@ class CudaEngine:
         if self._nf2ff is None:
             return None
         npts, nf = self._nf2ff
-        e = np.zeros(nf * npts * 6, np.float32)
-        h = np.zeros(nf * npts * 6, np.float32)
+        e = np.empty(nf * npts * 6, np.float32)       # filled whole by the call
+        h = np.empty(nf * npts * 6, np.float32)
         self._ck(self._lib.efs_read_nf2ff(self._h, _p(e, C.c_float), _p(h, C.c_float), e.size))
         if allFrequencies:
             return {"accumE": e.reshape(nf, npts * 6), "accumH": h.reshape(nf, npts * 6)}
