@@ -47,6 +47,98 @@ def openems_cavity():
                 probes=[probe], include_t0=True)
 
 
+def openems_dipole():
+    """The native-openEMS dipole fixture (reference
+    tests/generate_fixtures.py:313-423): a z-directed hard E source over one
+    dipole length L = lambda/50 at f_max = 1 GHz, on a uniform mesh of
+    step L/2 over +-20 L per axis (81 lines, drawing unit 1 um), Mur ABC on
+    all six faces, a Gaussian pulse (f0 = 0, fc = f_max), 500 steps at the
+    Courant step, and four field probes at the nodes nearest to (-+2.25 L, 0,
+    0), sampled every 21 steps from t = 0.
+
+    The hard source follows openEMS's hard E excitation: the source edges
+    get vv = vi = 0 (the update leaves them at zero) and the excitation
+    writes amplitude (edge length, E = 1 V/m along +z) x signal.  Mur faces are
+    listed face by face in openEMS's order (xmin, xmax, ymin, ymax, zmin,
+    zmax), each face's two tangential components after one another, so a
+    corner edge keeps the value of the last face as in openEMS.  Probes:
+    `field_probes` maps a probe name to (field, component, node, length):
+    the raw field at the node divided by its edge length (E: primal, H:
+    dual), which is what the fixture's probe files hold at these nodes."""
+    du, f_max = 1e-6, 1e9
+    lam = opgen.C0 / f_max / du
+    L = lam / 50
+    half, ext = L / 2, L * 20
+    vals = []                                   # the generator's accumulated line values (um)
+    v = -ext
+    while v <= ext + 0.001:
+        vals.append(v)
+        v += half
+    lines = [float("%.10e" % x) * du for x in vals]     # as written to the XML, in metres
+    mesh = opgen.Mesh(lines, lines, lines)
+    dT = opgen.cfl_dt(mesh)
+    vv, vi, ii, iv = opgen.operator_dense(mesh, dT, bc=(-1,) * 6)
+    Nx, Ny, Nz = mesh.shape
+    amp, dirs, pos = [], [], []
+    for n, (x, y, z) in opgen.find_path(mesh, [0.0, 0.0, -L / 2 * du], [0.0, 0.0, L / 2 * du]):
+        vv[n][x, y, z] = 0.0
+        vi[n][x, y, z] = 0.0
+        amp.append(mesh.dl(n)[(x, y, z)[n]])
+        dirs.append(n)
+        pos.append(x * Ny * Nz + y * Nz + z)
+    steps = 500
+    sig = opgen.gauss_signal(0.0, f_max, dT, steps)
+    faces = [(0, "lo"), (0, "hi"), (1, "lo"), (1, "hi"), (2, "lo"), (2, "hi")]
+    coeff, normal, shifted = [], [], []
+    for f in faces:
+        m = opgen.mur_dual(mesh, dT, [f])
+        for s in ("nyP", "nyPP"):
+            coeff.append(m["coeff_" + s])
+            normal.append(m["normal_idx_" + s])
+            shifted.append(m["shifted_idx_" + s])
+
+    def snap(val):                              # the generator's snap: first of the nearest lines
+        return min(range(len(vals)), key=lambda i: abs(vals[i] - val))
+    s = 4.5 * L / 2
+    node = lambda px: (snap(px), snap(0.0), snap(0.0))
+    dl2, dd1 = mesh.dl(2), mesh.dd(1)
+    probes = {}
+    for name, px in (("et1", -s), ("et2", s)):
+        p = node(px)
+        probes[name] = ("volt", 2, p, float(dl2[p[2]]))
+    for name, px in (("ht1", -s), ("ht2", s)):
+        p = node(px)
+        probes[name] = ("curr", 1, p, float(dd1[p[1]]))
+    return dict(name="openems_dipole", grid=list(mesh.shape), dT=dT, maxTS=steps, endCrit=0.0, mesh=mesh,
+                coefficients=dict(vv=opgen.flat(vv), vi=opgen.flat(vi), ii=opgen.flat(ii), iv=opgen.flat(iv)),
+                excitation=dict(signal=sig.astype(np.float32), delay=[0] * len(amp), amp=np.float32(amp), dir=dirs,
+                                pos=pos, period=0),
+                mur=dict(coeff=np.concatenate(coeff), normal_idx=np.concatenate(normal),
+                         shifted_idx=np.concatenate(shifted)),
+                field_probes=probes, sample_interval=21)
+
+
+def run_field_probes(engine, job):
+    """Configure `engine` with the job and sample its `field_probes` at
+    t = 0 and every `sample_interval` steps up to maxTS; returns
+    {name: float64 series}.  Reads whole fields (getFields), so it suits
+    small grids."""
+    configure(engine, job)
+    Nx, Ny, Nz = job["grid"]
+    N = Nx * Ny * Nz
+    out = {k: [] for k in job["field_probes"]}
+    step, k = job["sample_interval"], 0
+    while True:
+        f = engine.getFields()
+        for name, (field, n, (x, y, z), length) in job["field_probes"].items():
+            out[name].append(float(np.asarray(f[field]).reshape(-1)[n * N + x * Ny * Nz + y * Nz + z]) / length)
+        if k + step > job["maxTS"]:
+            break
+        engine.iterate(step)
+        k += step
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
 def openems_cavity_modes(steps=20000):
     """The native-openEMS cavity-resonator fixture (reference
     tests/generate_fixtures.py:63-178): 26x11x32 lines over 5x2x6 cm, PEC

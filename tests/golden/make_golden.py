@@ -14,6 +14,11 @@ The outputs are committed so the tests never read the reference tree.
   coax_ports.npz          coax/reference.json: port voltage and current series
                           (time_s, values), the analytic Z0 and the tolerance band
                           the reference's port test applies (tests/test_api.mjs:585-620)
+  openems_dipole.npz      dipole/probe_*.csv: the four field probes of the hard-source
+                          dipole with Mur on all faces (24 samples every 21 steps from
+                          t=0): all three components per probe (E probes et1/et2 in
+                          V/m, H probes ht1/ht2 in A/m), their sample times, the probe
+                          nodes of the file headers and the fixture's amplitude floors
 """
 import json
 import os
@@ -51,4 +56,31 @@ np.savez(os.path.join(OUT, "openems_cavity_modes.npz"),
          tolerances=np.asarray([cav["tolerances"][k] for k in ("te_freq_rel", "tm_freq_lower_rel", "te_min_amplitude",
                                                                "tm_min_amplitude")], np.float64),
          dims=np.asarray([cav["dimensions_m"][k] for k in ("a", "b", "d")], np.float64))
+
+
+def probe_csv(path):
+    """(node [i, j, k] of the header, rows of t and the three components)."""
+    node, rows = None, []
+    for line in open(path):
+        if line.startswith("%"):
+            if "start-coordinates" in line:
+                node = [int(v) for v in line.split("[")[1].split("]")[0].split(",")]
+            continue
+        if line.strip():
+            rows.append([float(v) for v in line.split()])
+    return node, np.asarray(rows, np.float64)
+
+
+dip = json.load(open(os.path.join(fx, "dipole", "reference.json")))
+arrays = {}
+for name in ("et1", "et2", "ht1", "ht2"):
+    node, rows = probe_csv(os.path.join(fx, "dipole", "probe_%s.csv" % name))
+    # the fixture's json keeps |field| per sample; the files hold the components
+    assert np.allclose(np.sqrt((rows[:, 1:] ** 2).sum(1)), dip["probe_" + name]["voltage"], rtol=1e-9, atol=0)
+    arrays[name + "_t"] = rows[:, 0]
+    arrays[name] = rows[:, 1:]
+    arrays[name + "_node"] = np.asarray(node, np.int64)
+tol = dip["tolerances"]
+np.savez(os.path.join(OUT, "openems_dipole.npz"), min_e_amp=np.float64(tol["min_e_amp"]),
+         min_h_amp=np.float64(tol["min_h_amp"]), **arrays)
 print("wrote", OUT)

@@ -5,6 +5,9 @@ a 16x8x18 PEC cavity from openEMS's basic/sse/sse-compressed engines (bit
 identical).  The operator generator plus the oracle reproduce it within the
 1e-4 relative L2 bar in every arithmetic mode; this pins the oracle, the
 generator's EC-FDTD conventions and the probe timing to native openEMS.
+The cavity-resonator fixture pins the Courant step and long runs; the dipole
+fixture (hard source, Mur on all six faces, E and H field probes) pins the
+Mur ABC and the H sampling.
 """
 import json
 import os
@@ -104,3 +107,45 @@ def test_cavity_mode_frequencies():
         peaks = [i for i in range(1, len(s) - 1) if s[i] > s[i - 1] and s[i] > s[i + 1] and s[i] > 0.2]
         for i in peaks:
             assert min(abs(f[i] - fa) / fa for fa in analytic) < 0.01, f[i]
+
+
+# ---- the dipole fixture (tests/fixtures/dipole of the reference) ----
+
+def test_dipole_job_matches_fixture_setup():
+    """Grid, probe nodes and sample times of workloads.openems_dipole against
+    the fixture's probe files (header nodes, t column)."""
+    g = np.load(os.path.join(GOLD, "openems_dipole.npz"))
+    job = workloads.openems_dipole()
+    assert job["grid"] == [81, 81, 81]
+    assert list(job["excitation"]["dir"]) == [2, 2]                 # two Ez edges across the centre node
+    assert list(job["excitation"]["pos"]) == [40 * 81 * 81 + 40 * 81 + 39, 40 * 81 * 81 + 40 * 81 + 40]
+    for name, (field, n, node, length) in job["field_probes"].items():
+        assert list(node) == [int(v) for v in g[name + "_node"]], name
+    dT = job["dT"]
+    assert abs(g["et1_t"][1] - 21 * dT) < 1e-7 * 21 * dT         # E sampled every 21 steps from t = 0
+    assert abs(g["ht1_t"][0] - dT / 2) < 1e-7 * dT               # H half a step later
+    assert len(g["et1_t"]) == 24
+
+
+@pytest.mark.parametrize("mode", ["f32", "js", "f64"])
+def test_dipole_probes_match_native_openems(mode):
+    """Hard-source dipole with Mur on all six faces, 500 steps: Ez at the two E
+    probes and Hy at the two H probes (the fields' only non-noise components
+    on the x axis) within 1e-4 relative L2 of native openEMS in every
+    arithmetic mode (measured 4e-7 .. 1.2e-5).  This pins the Mur ABC, the
+    hard source and the probe sampling.  Also the reference's own checks on
+    this fixture (tests/test_wasm.mjs:303-360): amplitude floors and the
+    symmetry of the two sides."""
+    g = np.load(os.path.join(GOLD, "openems_dipole.npz"))
+    job = workloads.openems_dipole()
+    got = workloads.run_field_probes(OracleEngine(mode=mode), job)
+    for name, comp in (("et1", 2), ("et2", 2), ("ht1", 1), ("ht2", 1)):
+        ref = g[name][:, comp]
+        assert got[name].shape == ref.shape
+        err = np.linalg.norm(got[name] - ref) / np.linalg.norm(ref)
+        assert err < 1e-4, (name, err)
+    assert min(np.abs(got["et1"]).max(), np.abs(got["et2"]).max()) >= g["min_e_amp"]
+    assert min(np.abs(got["ht1"]).max(), np.abs(got["ht2"]).max()) >= g["min_h_amp"]
+    for a, b in (("et1", "et2"), ("ht1", "ht2")):
+        ra, rb = np.abs(got[a]).max(), np.abs(got[b]).max()
+        assert max(ra, rb) / min(ra, rb) < 10
