@@ -47,10 +47,15 @@ typedef struct efs_engine efs_engine;
 /* --- lifetime ---------------------------------------------------------- */
 
 /* WebGPUEngine.initGPU (:1107-1135): bind a device, create the stream.
- * Returns EFS_ERR_CUDA when no device is usable (the reference returns false). */
+ * Returns EFS_ERR_CUDA when no device is usable (the reference returns false).
+ * Each engine's pinned host words (the status word its kernels report a
+ * timed-out wait through, two energy result slots: 32 bytes) come from
+ * mapped pinned pages of 4 KB that the library keeps for the life of the
+ * process and hands to later engines after efs_destroy. */
 efs_status efs_create(efs_engine** out, int device);
 
-/* WebGPUEngine.destroy (:3163-3227). Safe on NULL. */
+/* WebGPUEngine.destroy (:3163-3227): waits for the engine's stream, frees its
+ * device memory and graphs.  Safe on NULL. */
 efs_status efs_destroy(efs_engine* e);
 
 /* Message of the last failing call on this engine (or of the last failing
