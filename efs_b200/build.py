@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libefs.so")
 SOURCES = ["efs_engine.cu"]
-HEADERS = ["efs_kernels.cuh", "efs_fused.cuh", "efs_tma.cuh", "efs_batch.cuh", os.path.join("..", "..", "include", "efs.h")]
+HEADERS = ["efs_kernels.cuh", "efs_fused.cuh", "efs_tma.cuh", "efs_batch.cuh", "efs_host.h", os.path.join("..", "..", "include", "efs.h")]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
