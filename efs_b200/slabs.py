@@ -27,7 +27,11 @@ Ny x Nz floats per interface and timestep; PBC along x would couple the
 first and last ranks and is rejected.
 
 Sampling outputs (NF2FF surface points, probes) are assigned to the rank
-that owns their plane; energies are sums over owned planes.
+that owns their plane; energies are sums over owned planes.  The whole-solve
+results are reductions over ranks: the energy (one scalar), the radiated
+power through the NF2FF surface (one scalar) and the far field (E_theta and
+E_phi per angle are sums over surface points, so each rank evaluates its own
+points and the complex components are summed; P_rad is formed after the sum).
 """
 import numpy as np
 
@@ -151,6 +155,10 @@ def split(job, world):
                                 primalEdgeLens=[np.asarray(nf["primalEdgeLens"][0])[g0:g1]] + list(nf["primalEdgeLens"][1:]),
                                 dualEdgeLens=[np.asarray(nf["dualEdgeLens"][0])[g0:g1]] + list(nf["dualEdgeLens"][1:]))
             sub["nf2ff_points"] = np.flatnonzero(k)          # positions in the job's point list
+            if job.get("nf2ff_meta") is not None:            # far-field rows of the owned points (global positions)
+                sub["nf2ff_meta"] = np.asarray(job["nf2ff_meta"], np.float32).reshape(-1, 8)[k].ravel()
+            if job.get("nf2ff_freqs") is not None:
+                sub["nf2ff_freqs"] = job["nf2ff_freqs"]
         out.append((s, sub))
     return out
 
@@ -205,6 +213,57 @@ def exchange_dist(slab, world, get_planes, set_planes, send_recv):
         set_planes(r, slab["x1"] - slab["g0"], got[0], got[1])
 
 
+# ---------------------------------------------------------------------------
+# Reductions over ranks.  `all_reduce_sum(x)` returns the sum over ranks of a
+# float or float64 array (torch.distributed.all_reduce in a process group, a
+# plain sum when one process drives every slab); every rank calls it in the
+# same order.
+# ---------------------------------------------------------------------------
+Z0 = 376.73031346177066              # free-space impedance used by the far field (efs_kernels.cuh)
+
+
+def owned_energy(volt, curr, slab, grid):
+    """This rank's share of the single-domain energy: the sum of volt^2 +
+    curr^2 over cells x < Nx-1, y < Ny-1, z < Nz-1 and the three components
+    (src/webgpu-engine.mjs:3090-3103), over the owned planes, in f64.
+    volt, curr: the owned planes, (3, x1 - x0, Ny*Nz) as getPlanes returns."""
+    Nx, Ny, Nz = grid
+    n = min(slab["x1"], Nx - 1) - slab["x0"]
+    if n <= 0 or Ny < 2 or Nz < 2:
+        return 0.0
+    tot = 0.0
+    for a in (volt, curr):
+        b = np.asarray(a).reshape(3, -1, Ny, Nz)[:, :n, :Ny - 1, :Nz - 1].astype(np.float64)
+        tot += float(np.sum(b * b))
+    return tot
+
+
+def energy_dist(volt, curr, slab, grid, all_reduce_sum):
+    """Energy of the decomposed solve: the owned shares summed over ranks
+    (one scalar all-reduce)."""
+    return float(all_reduce_sum(np.float64(owned_energy(volt, curr, slab, grid))))
+
+
+def far_field_dist(partial, all_reduce_sum):
+    """Far field of the decomposed solve from each rank's far field of its
+    own NF2FF points (the engine's computeNF2FFfarField with the rank's
+    accumulators and point rows, the same angles, frequency, centre and
+    radius): (n_angles, 5) rows [P_rad, E_theta re, im, E_phi re, im].
+    E_theta and E_phi are sums over surface points, so the ranks' complex
+    components add (one all-reduce of 4 values per angle) and P_rad =
+    (|E_theta|^2 + |E_phi|^2) / (2 Z0) is formed from the sums."""
+    p = np.asarray(partial, np.float64).reshape(-1, 5)
+    e = np.asarray(all_reduce_sum(np.ascontiguousarray(p[:, 1:5])), np.float64)
+    return np.column_stack([(e * e).sum(axis=1) / (2 * Z0), e])
+
+
+def rad_power_dist(accE, accH, meta, all_reduce_sum):
+    """Radiated power through the NF2FF surface (sim-engine.mjs:474-497),
+    a sum over surface points: each rank's points, summed over ranks."""
+    from .opgen import rad_power
+    return float(all_reduce_sum(np.float64(rad_power(accE, accH, meta) if len(meta) else 0.0)))
+
+
 class LocalSlabs:
     """Every slab of a job on engines driven by this process (one GPU each,
     or several on one GPU): configure, step and exchange ghost planes with
@@ -242,6 +301,15 @@ class LocalSlabs:
             vs.append(v)
             cs.append(c)
         return np.concatenate(vs, axis=1), np.concatenate(cs, axis=1)
+
+    def energy(self):
+        """Energy of the whole grid from the owned planes (energy_dist with a
+        plain sum over the slabs)."""
+        tot = 0.0
+        for (s, _), e in zip(self.parts, self.engines):
+            v, c = e.getPlanes(s["x0"] - s["g0"], s["x1"] - s["x0"])
+            tot += owned_energy(v, c, s, self.job["grid"])
+        return tot
 
     def destroy(self):
         for e in self.engines:

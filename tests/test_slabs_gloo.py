@@ -7,7 +7,10 @@ solve bit for bit (without the exchange they do not).  Two jobs: the large plain
 dispersive workload at 36x24x28 (UPML on all faces, so the x slabs cut UPML
 regions; Drude/Lorentz spheres with the ADE apply step; TFSF at 30 degrees).
 World size 2 over gloo (send/recv between processes) and world size 3 in one
-process (the middle rank has both neighbours)."""
+process (the middle rank has both neighbours).  The whole-solve results are
+reductions over the ranks (efs_b200.slabs: energy, radiated power and far
+field, summed by all-reduce over gloo or by a plain sum in one process) and
+must equal the single-domain values up to f64 summation order."""
 import os
 import socket
 import tempfile
@@ -85,6 +88,45 @@ def _check(job, slabs, results):
         assert seen == npts
 
 
+ANGLES = (np.deg2rad(np.arange(0.0, 181.0, 30.0)).astype(np.float32),
+          np.deg2rad(np.arange(0.0, 360.0, 45.0)).astype(np.float32))
+
+
+def _partials(o, s, sub, get):
+    """This rank's owned planes, far field of its own NF2FF points at
+    frequency 0 and its NF2FF accumulators/rows (for the radiated power)."""
+    from oracle.oracle import far_field
+    v, c = get(s["rank"], s["x0"] - s["g0"], s["x1"] - s["x0"])
+    A = ANGLES[0].size * ANGLES[1].size
+    if sub.get("nf2ff") and sub["nf2ff"]["numPoints"]:
+        acc = o.readNF2FFAccumulation(True)
+        aE, aH = np.asarray(acc["accumE"])[0], np.asarray(acc["accumH"])[0]
+        ff = far_field(aE, aH, sub["nf2ff_meta"], *ANGLES, sub["nf2ff_freqs"][0])
+        meta = np.asarray(sub["nf2ff_meta"], np.float32)
+    else:
+        aE = aH = meta = np.zeros(0, np.float32)
+        ff = np.zeros((A, 5))
+    return v, c, ff, aE, aH, meta
+
+
+def _check_reductions(job, reduced):
+    """reduced = (energy, far field (A, 5), radiated power) of the slabs
+    against the single-domain oracle: f64 sums in another order."""
+    from efs_b200 import opgen
+    from oracle.oracle import far_field
+    o = _single(job)
+    energy, ff, prad = reduced
+    assert abs(energy - o.energy()) <= 1e-12 * abs(o.energy()), (energy, o.energy())
+    acc = o.readNF2FFAccumulation(True)
+    aE, aH = np.asarray(acc["accumE"])[0], np.asarray(acc["accumH"])[0]
+    ref = far_field(aE, aH, job["nf2ff_meta"], *ANGLES, job["nf2ff_freqs"][0])
+    scale = np.abs(ref[:, 1:]).max()
+    assert np.abs(ff[:, 1:] - ref[:, 1:]).max() <= 1e-9 * scale
+    assert np.abs(ff[:, 0] - ref[:, 0]).max() <= 1e-9 * ref[:, 0].max()
+    p_ref = opgen.rad_power(aE, aH, job["nf2ff_meta"])
+    assert abs(prad - p_ref) <= 1e-9 * abs(p_ref), (prad, p_ref)
+
+
 def _rank_results(o, s, sub, Ny, Nz):
     from efs_b200 import slabs
     f = o.getFields()
@@ -117,6 +159,12 @@ def test_three_slabs_in_process(name):
         slabs.exchange([s for s, _ in parts], get, put)
     results = {s["rank"]: _rank_results(engines[s["rank"]], s, sub, Ny, Nz) for s, sub in parts}
     _check(job, [s for s, _ in parts], results)
+    # whole-solve results as reductions over the slabs (a plain sum in one process)
+    parts_r = [_partials(engines[s["rank"]], s, sub, get) for s, sub in parts]
+    energy = sum(slabs.owned_energy(v, c, s, job["grid"]) for (s, _), (v, c, *_r) in zip(parts, parts_r))
+    ff = slabs.far_field_dist(parts_r[0][2], lambda x: sum(np.asarray(p[2])[:, 1:5] for p in parts_r))
+    prad = sum(slabs.rad_power_dist(p[3], p[4], p[5], lambda x: x) for p in parts_r)
+    _check_reductions(job, (energy, ff, prad))
 
 
 def _slab_rank(rank, world, port, outdir, name):
@@ -153,6 +201,16 @@ def _slab_rank(rank, world, port, outdir, name):
         slabs.exchange_dist(s, world, get, put, send_recv)
     res = _rank_results(o, s, sub, Ny, Nz)
     np.savez(os.path.join(outdir, "rank%d.npz" % rank), *res)
+
+    def all_reduce_sum(x):
+        t = torch.from_numpy(np.array(x, np.float64).reshape(-1))
+        dist.all_reduce(t)
+        return t.numpy().reshape(np.shape(x))
+    v, c, ff, aE, aH, meta = _partials(o, s, sub, get)
+    energy = slabs.energy_dist(v, c, s, job["grid"], all_reduce_sum)
+    ff = slabs.far_field_dist(ff, all_reduce_sum)
+    prad = slabs.rad_power_dist(aE, aH, meta, all_reduce_sum)
+    np.savez(os.path.join(outdir, "reduced%d.npz" % rank), energy=energy, ff=ff, prad=prad)
     dist.destroy_process_group()
 
 
@@ -168,3 +226,7 @@ def test_two_slabs_over_gloo(name):
         z = np.load(os.path.join(out, "rank%d.npz" % s["rank"]))
         results[s["rank"]] = [z["arr_%d" % i] for i in range(5)]
     _check(job, [s for s, _ in parts], results)
+    red = [np.load(os.path.join(out, "reduced%d.npz" % s["rank"])) for s, _ in parts]
+    for z in red[1:]:                      # every rank holds the same reduced results
+        assert float(z["energy"]) == float(red[0]["energy"]) and np.array_equal(z["ff"], red[0]["ff"])
+    _check_reductions(job, (float(red[0]["energy"]), red[0]["ff"], float(red[0]["prad"])))
