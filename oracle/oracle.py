@@ -184,6 +184,21 @@ class OracleEngine:
         self.write("volt", volt)
         self.write("curr", curr)
 
+    def getPlanes(self, x, count):
+        """x-planes [x, x+count) of E and H as (3, count, Ny*Nz) float32 (the
+        engine's getPlanes, through whole-field reads: small grids only)."""
+        nx, ny, nz = self.numLines
+        v = np.asarray(self.read("volt"), np.float32).reshape(3, nx, ny * nz)[:, x:x + count].copy()
+        c = np.asarray(self.read("curr"), np.float32).reshape(3, nx, ny * nz)[:, x:x + count].copy()
+        return v, c
+
+    def setPlanes(self, x, volt, curr):
+        nx, ny, nz = self.numLines
+        for name, a in (("volt", volt), ("curr", curr)):
+            f = np.asarray(self.read(name), np.float32).reshape(3, nx, ny * nz).copy()
+            f[:, x:x + a.shape[1]] = a
+            self.write(name, f.reshape(-1))
+
     # --- configure* (reference argument objects) -------------------------
     def configureExcitation(self, exc):
         sig, amp = _f32(exc["signal"]), _f32(exc["amp"])

@@ -230,3 +230,21 @@ def test_two_slabs_over_gloo(name):
     for z in red[1:]:                      # every rank holds the same reduced results
         assert float(z["energy"]) == float(red[0]["energy"]) and np.array_equal(z["ff"], red[0]["ff"])
     _check_reductions(job, (float(red[0]["energy"]), red[0]["ff"], float(red[0]["prad"])))
+
+
+def test_local_slabs_driver():
+    """slabs.LocalSlabs (the in-process driver the GPU runs use) on the
+    oracle: owned fields bit-exact against one domain, energy() equal up to
+    f64 summation order."""
+    from efs_b200 import slabs
+    from oracle.oracle import OracleEngine
+    job = _job("plain")
+    Nx, Ny, Nz = job["grid"]
+    ls = slabs.LocalSlabs(job, 3, lambda r: OracleEngine(mode="f32"))
+    ls.iterate(STEPS)
+    v, c = ls.owned_fields()
+    o = _single(job)
+    assert np.array_equal(v.view(np.uint32), np.asarray(o.volt, np.float32).reshape(3, Nx, Ny * Nz).view(np.uint32))
+    assert np.array_equal(c.view(np.uint32), np.asarray(o.curr, np.float32).reshape(3, Nx, Ny * Nz).view(np.uint32))
+    assert abs(ls.energy() - o.energy()) <= 1e-12 * o.energy()
+    ls.destroy()
