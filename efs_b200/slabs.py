@@ -195,17 +195,17 @@ def exchange(ranks, get_planes, set_planes, send=None):
 def exchange_dist(slab, world, get_planes, set_planes, send_recv):
     """The ghost exchange of one rank in a process group: send_recv(dst, arrays, src, shapes)
     posts the sends to `dst` and receives from `src` (None: no partner).  Every rank
-    takes the same two rounds in the same order: first upward (last owned plane to
+    takes the same two exchanges in the same order: first upward (last owned plane to
     rank + 1), then downward (first owned planes to rank - 1)."""
     r = slab["rank"]
     lo_ghost = slab["x0"] - slab["g0"]                          # count of lower ghost planes held
     hi_ghost = slab["g1"] - slab["x1"]
-    # round 1: plane x1-1 up; receive plane x0-1 from below
+    # first exchange: plane x1-1 up; receive plane x0-1 from below
     out = get_planes(r, slab["x1"] - 1 - slab["g0"], 1) if r + 1 < world else None
     got = send_recv(r + 1 if r + 1 < world else None, out, r - 1 if r > 0 else None, 1)
     if got is not None and lo_ghost:
         set_planes(r, 0, got[0], got[1])
-    # round 2: planes x0, x0+1 down; receive planes x1, x1+1 from above
+    # second exchange: planes x0, x0+1 down; receive planes x1, x1+1 from above
     cnt_down = min(GHOST_HI, slab["x1"] - slab["x0"])
     out = get_planes(r, slab["x0"] - slab["g0"], cnt_down) if r > 0 else None
     got = send_recv(r - 1 if r > 0 else None, out, r + 1 if r + 1 < world else None, hi_ghost)

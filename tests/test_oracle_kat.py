@@ -3,7 +3,7 @@
 Each test restates a section of tests/test_webgpu.mjs (line numbers cited) and
 runs in all three arithmetic modes of the oracle (f32 = the CUDA engine's
 order, js = the reference CPUFDTDEngine's f64-intermediate / f32-storage
-arithmetic, f64).  These pin the oracle before it is used to judge the CUDA
+arithmetic, f64).  These pin the oracle before it is used to check the CUDA
 engine.
 """
 import math
