@@ -237,6 +237,9 @@ def large_plain(n=512, delta=0.5e-3, seed=2, nboxes=40, pml=8, nfreq=3, tfsf_ins
     pec_boxes, diel = [], []
     margin = tfsf_inset + 4
     lo_cap = max(margin, 1)
+    if nboxes and n <= lo_cap + 1:
+        raise ValueError("large_plain: n = %d leaves no room for boxes inside the TFSF inset %d (need n > %d)"
+                         % (n, tfsf_inset, lo_cap + 1))
     for i in range(nboxes):
         size = rng.integers(max(2, n // 32), max(3, n // 8), 3)
         lo = np.array([rng.integers(lo_cap, max(lo_cap + 1, nc - margin - s)) for s in size])
