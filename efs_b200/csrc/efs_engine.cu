@@ -963,7 +963,9 @@ void alloc_fields(efs_engine* e, const uint32_t dims[3]) {
     const size_t Nd = (size_t)dims[0] * dims[1] * Pz;
     if (3 * Nd >= (1ull << 32))
         fail(EFS_ERR_RANGE, "grid too large for 32-bit field indices (3*Nx*Ny*Pz >= 2^32, Pz = Nz rounded up to a multiple of 4)");
-    // a fresh init drops every extension
+    // a fresh init drops every extension; the engine counts as initialised
+    // again only when the init call completes (a failed init leaves it unusable)
+    e->inited = false;
     e->drop_graphs();
     e->pml.clear();
     e->exc_on = e->mur_on = e->tfsf_on = e->ade_on = e->rlc_on = e->ss_on = e->pbc_on = e->ring_on = e->nf_on = false;

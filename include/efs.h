@@ -75,7 +75,9 @@ efs_status efs_init(efs_engine* e, const uint32_t dims[3],
  * u32) indexes rows of `table` (ntable rows of 12 floats:
  * vv_x vv_y vv_z vi_x vi_y vi_z ii_x ii_y ii_z iv_x iv_y iv_z).
  * No counterpart in the reference (it always ships dense arrays); used by
- * operator generators that know the material of each cell. */
+ * operator generators that know the material of each cell.  An index >=
+ * ntable returns EFS_ERR_INVALID (checked on the device after the upload)
+ * and leaves the engine uninitialised. */
 efs_status efs_init_indexed(efs_engine* e, const uint32_t dims[3],
                             const uint32_t* mat, const float* table, uint32_t ntable);
 

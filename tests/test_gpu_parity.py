@@ -631,6 +631,17 @@ def test_invalid_inputs_raise(cuda_engine_cls):
         g.configurePML([pml_region((2, 0, 0), (3, 4, 4), 1)])
     g.iterate(2)                          # engine still usable
     assert g.numTS == 2
+    mat = np.zeros(4 * 4 * 4, np.uint32)
+    mat[10] = 2
+    with pytest.raises(EfsError):
+        g.init(N, dict(mat=mat, table=np.ones((2, 12), np.float32)))     # index 2 of a 2-row table
+    with pytest.raises(EfsError):
+        g.iterate(1)                      # a failed init leaves the engine uninitialised
+    mat[10] = 1
+    g.init(N, dict(mat=mat, table=np.full((2, 12), 0.5, np.float32)))
+    g.iterate(2)
+    assert g.numTS == 2
+    g.destroy()
 
 
 def test_openems_cavity_fixture_on_gpu(cuda_engine_cls):
