@@ -441,3 +441,74 @@ def test_far_field_infinitesimal_dipole():  # tests/test_api.mjs:1694-1786
     prad = (P * np.sin(theta)[:, None]).sum() * (math.pi / (nt - 1)) * (2 * math.pi / (nph - 1))
     dmax = 4 * math.pi * P.max() / prad
     assert abs(dmax - 1.5) / 1.5 < 0.10, dmax
+
+
+# order of the reference's timestep (tests/test_webgpu.mjs:2675-2776)
+STEP_ORDER = ["accumulateEnergy", "preVoltageUpdatePML", "updateVoltADE", "murPreVoltage", "preVoltageRLC",
+              "updateVoltages", "postVoltageUpdatePML", "applyTFSFVoltage", "murPostVoltage", "applyExcitation",
+              "murApply", "applyRLC", "preCurrentUpdatePML", "updateCurrADE", "updateCurrents",
+              "postCurrentUpdatePML", "applyTFSFCurrent"]
+
+
+def _all_extensions(N, seed=11):
+    """f32 oracle with every extension, their targets overlapping: UPML slab
+    z = 0..1, Lorentz ADE on UPML and interior cells, Mur on the z = Nz-1 face,
+    excitation, TFSF and RLC on Mur and UPML cells, a steady-state probe in
+    the UPML slab; random fields."""
+    r = np.random.default_rng(seed)
+    Nx, Ny, Nz = N
+    e = OracleEngine(N, free_space(*N), mode="f32")
+    cell = lambda x, y, z: x * Ny * Nz + y * Nz + z
+    t = 3 * Nx * Ny * 2
+    u = lambda lo, hi: r.uniform(lo, hi, t)
+    e.configurePML([dict(startPos=[0, 0, 0], numLines=[Nx, Ny, 2], vv=u(0.6, 1.0), vvfo=u(0.0, 0.3), vvfn=u(0.8, 1.2),
+                         ii=u(0.6, 1.0), iifo=u(0.0, 0.3), iifn=u(0.8, 1.2))])
+    lp = [cell(2, 2, 1), cell(3, 2, 3), cell(2, 3, Nz - 1)]
+    e.configureLorentz({"orders": [dict(numCells=len(lp), hasLorentz=True, directions=[dict(
+        dir=n, pos_idx=lp, v_int_ADE=[0.9, 0.8, 0.7], v_ext_ADE=[0.2, 0.1, 0.3], v_Lor_ADE=[0.1, 0.2, 0.05],
+        i_int_ADE=[0.85, 0.9, 0.6], i_ext_ADE=[0.1, 0.2, 0.1], i_Lor_ADE=[0.05, 0.1, 0.2]) for n in range(3)])]})
+    normal = [n * Nx * Ny * Nz + cell(x, y, Nz - 1) for n in (0, 1) for x in range(Nx) for y in range(Ny)]
+    shifted = [n * Nx * Ny * Nz + cell(x, y, Nz - 2) for n in (0, 1) for x in range(Nx) for y in range(Ny)]
+    e.configureMur(dict(coeff=0.3, normal_idx=normal, shifted_idx=shifted))
+    e.configureExcitation(dict(signal=(0.5 + np.sin(np.arange(8) * 0.7)).astype(np.float32), delay=[0, 1], amp=[0.7, -0.4],
+                               dir=[0, 2], pos=[cell(2, 3, Nz - 1), cell(3, 3, 1)], period=0))
+    vp = [dict(field_idx=0 * Nx * Ny * Nz + cell(2, 3, Nz - 1), delay_int=0, delay_frac=0.25, amp=0.5),
+          dict(field_idx=1 * Nx * Ny * Nz + cell(3, 2, Nz - 2), delay_int=0, delay_frac=0.5, amp=-0.3),
+          dict(field_idx=2 * Nx * Ny * Nz + cell(2, 2, 1), delay_int=0, delay_frac=0.0, amp=0.8)]
+    cp = [dict(field_idx=1 * Nx * Ny * Nz + cell(2, 2, 1), delay_int=0, delay_frac=0.75, amp=0.4),
+          dict(field_idx=0 * Nx * Ny * Nz + cell(3, 3, Nz - 2), delay_int=0, delay_frac=0.0, amp=0.6)]
+    e.configureTFSF(dict(signal=np.cos(np.arange(8) * 0.5).astype(np.float32), period=0, voltagePoints=vp,
+                         currentPoints=cp))
+    e.configureRLC(dict(elements=[
+        _rlc(field_idx=cell(2, 3, Nz - 1), direction=0, type_flag=0, i2v=0.1, ilv=0.2),
+        _rlc(field_idx=cell(3, 3, 1), direction=2, type_flag=1, i2v=0.2, ilv=0.1, vvd=0.5, vv2=0.1, vj1=0.2,
+             vj2=0.1, ib0=0.3, b1=0.2, b2=0.1)]))
+    e.configureSteadyState(dict(probe_idx=[2 * Nx * Ny * Nz + cell(2, 2, 1)], periodSamples=4, threshold=1e-6))
+    e.setSteadyState(True, 0)
+    tot = 3 * Nx * Ny * Nz
+    e.uploadFields(r.standard_normal(tot).astype(np.float32), r.standard_normal(tot).astype(np.float32))
+    return e
+
+
+def test_step_follows_the_reference_phase_order():  # tests/test_webgpu.mjs:2675-2776
+    """One step of the oracle equals the reference's 17 phases run one by one
+    in its order (the C++ extension priorities), bit for bit, with every
+    extension acting on shared cells; the same phases with the excitation and
+    the Mur apply swapped do not, so the comparison sees the order."""
+    N = (6, 6, 6)
+    a, b, c = _all_extensions(N), _all_extensions(N), _all_extensions(N)
+    a.step()
+    for name in STEP_ORDER:
+        b.phase(name)
+    swapped = list(STEP_ORDER)
+    i, j = swapped.index("applyExcitation"), swapped.index("murApply")
+    swapped[i], swapped[j] = swapped[j], swapped[i]
+    for name in swapped:
+        c.phase(name)
+    for f in ("volt", "curr"):
+        assert np.array_equal(np.asarray(a.read(f), np.float32).view(np.uint32),
+                              np.asarray(b.read(f), np.float32).view(np.uint32)), f
+    for f in ("ss_e1", "pml_volt_flux", "pml_curr_flux", "ade_volt", "ade_curr"):
+        assert np.array_equal(np.asarray(a.read(f)), np.asarray(b.read(f))), f
+    assert a.numTS == 1
+    assert not np.array_equal(np.asarray(a.read("volt")), np.asarray(c.read("volt")))
